@@ -1,0 +1,67 @@
+"""Builds ``libgargantua_gpu.so`` in-tree for sm_100a with nvcc.
+
+    python -m gargantua_b200.build [--verbose]
+
+``--verbose`` adds ``-Xptxas -v`` (registers, spills and shared memory per
+kernel).  Host code is built with ``-ffp-contract=off`` so the per-render
+constants it evaluates round exactly like the reference's Rust code.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+CSRC = PKG / "csrc"
+OUT = PKG / "libgargantua_gpu.so"
+SOURCES = ["gg_trace.cu", "gg_capi.cpp"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and Path(cand).exists():
+            return cand
+    raise FileNotFoundError("nvcc not found")
+
+
+def flags(verbose: bool = False) -> list[str]:
+    f = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-shared", "--expt-relaxed-constexpr",
+                "-Xcompiler", "-fPIC,-fvisibility=hidden,-ffp-contract=off,-O2",
+                "-I", str(PKG.parent / "include")]
+    if verbose:
+        f += ["-Xptxas", "-v"]
+    return f
+
+
+def build(verbose: bool = False, force: bool = False) -> Path:
+    srcs = [CSRC / s for s in SOURCES]
+    deps = srcs + list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + \
+        [PKG.parent / "include" / "gargantua_gpu.h"]
+    if not force and OUT.exists() and not verbose:
+        newest = max(p.stat().st_mtime for p in deps)
+        if OUT.stat().st_mtime >= newest:
+            return OUT
+    with tempfile.TemporaryDirectory() as tmp:
+        tmp_out = Path(tmp) / OUT.name
+        cmd = [nvcc()] + flags(verbose) + [str(s) for s in srcs] + ["-o", str(tmp_out)]
+        res = subprocess.run(cmd, capture_output=True, text=True)
+        if verbose or res.returncode != 0:
+            sys.stderr.write(res.stdout + res.stderr)
+        if res.returncode != 0:
+            raise RuntimeError(f"nvcc failed ({res.returncode}): {' '.join(cmd)}")
+        shutil.move(str(tmp_out), OUT)
+    return OUT
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--verbose", action="store_true")
+    ap.add_argument("--force", action="store_true")
+    a = ap.parse_args()
+    print(build(a.verbose, a.force))

@@ -1,0 +1,629 @@
+// gg_capi.cpp -- the C ABI of libgargantua_gpu.so (include/gargantua_gpu.h).
+//
+// Host side of a render: validate the public POD structs, evaluate the
+// per-render constants in the reference's operation order (camera frame,
+// metric at the camera, horizon), manage the context's device scratch, and
+// enqueue the trace kernels on the context's stream.  No function here
+// aborts, throws across the ABI or falls back to the CPU.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+
+#include "../../include/gargantua_gpu.h"
+#include "gg_launch.h"
+#include "gg_params.h"
+
+using gg::DevControl;
+using gg::DevOutputs;
+using gg::DevParams;
+
+struct gg_ctx {
+  int device = 0;
+  int sms = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev_start = nullptr, ev_stop = nullptr, ev_done = nullptr;
+  DevControl* ctl = nullptr;       // device counters
+  DevControl* ctl_host = nullptr;  // pinned mirror
+  void* samples = nullptr;         // per-sample linear colours (supersampling)
+  size_t samples_cap = 0;
+  void* staging = nullptr;         // device outputs of the host-buffer entry point
+  size_t staging_cap = 0;
+  bool pending = false;            // stats of the last device-pointer render not read yet
+  gg_stats_t last{};
+  std::mutex mu;
+};
+
+namespace {
+
+constexpr double kPi = 3.14159265358979323846;
+
+// ---- reference-order host math (no contraction: built -ffp-contract=off) --
+struct V3 {
+  double x, y, z;
+};
+double dot3(V3 a, V3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+V3 normalize3(V3 v) {
+  const double n = std::sqrt(dot3(v, v));
+  return {v.x / n, v.y / n, v.z / n};
+}
+V3 cross3(V3 a, V3 b) {
+  return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+
+struct G5 {
+  double tt, rr, thth, phph, tph;
+};
+
+// Schwarzschild::metric_tensor (schwarzschild.rs:26-43) and
+// Kerr::metric_tensor (kerr.rs:61-94), evaluated at the camera.
+G5 metric_at(const gg_metric_t& m, const double pos[4]) {
+  G5 g{};
+  double r = std::fmax(pos[1], 1e-10);
+  const double theta = pos[2];
+  if (m.kind == GG_METRIC_KERR) {
+    const double M = m.mass, a = m.spin, a2 = a * a;
+    const double ct = std::cos(theta);
+    const double sigma = r * r + a * a * ct * ct;
+    const double delta = r * r - 2.0 * M * r + a * a;
+    const double st = std::sin(theta);
+    const double sin2 = st * st;
+    g.tt = -(1.0 - 2.0 * M * r / sigma);
+    g.rr = sigma / delta;
+    g.thth = sigma;
+    g.phph = (r * r + a2 + 2.0 * M * a2 * r * sin2 / sigma) * sin2;
+    g.tph = -2.0 * M * a * r * sin2 / sigma;
+  } else {
+    const double rs = 2.0 * m.mass;
+    const double f = 1.0 - rs / r;
+    const double st = std::sin(theta);
+    g.tt = -f;
+    g.rr = 1.0 / f;
+    g.thth = r * r;
+    g.phph = r * r * st * st;
+    g.tph = 0.0;
+  }
+  return g;
+}
+
+bool finite_all(const double* p, int n) {
+  for (int i = 0; i < n; ++i)
+    if (!std::isfinite(p[i])) return false;
+  return true;
+}
+
+uint32_t spp_of(const gg_render_opts_t& o) {
+  if (o.jitter_spp > 0) return o.jitter_spp;
+  const uint32_t spa = o.samples_per_axis < 1 ? 1 : o.samples_per_axis;
+  return spa * spa;
+}
+
+int validate(const gg_metric_t* metric, const gg_camera_t* camera, const gg_disk_t* disk,
+             const gg_integrator_t* integ, const gg_render_opts_t* opts, uint32_t width,
+             uint32_t height) {
+  if (!metric || !camera || !integ || !opts) return GG_ERR_INVALID_ARG;
+  if (metric->kind != GG_METRIC_SCHWARZSCHILD && metric->kind != GG_METRIC_KERR)
+    return GG_ERR_INVALID_ARG;
+  if (!(std::isfinite(metric->mass) && metric->mass > 0.0)) return GG_ERR_INVALID_ARG;
+  if (metric->kind == GG_METRIC_KERR &&
+      !(std::isfinite(metric->spin) && std::fabs(metric->spin) <= metric->mass))
+    return GG_ERR_INVALID_ARG;
+  if (!finite_all(camera->position, 4) || !finite_all(camera->look_at, 3) ||
+      !finite_all(camera->up, 3))
+    return GG_ERR_INVALID_ARG;
+  if (!(camera->aspect > 0.0 && std::isfinite(camera->aspect))) return GG_ERR_INVALID_ARG;
+  if (!(camera->fov_y_radians > 0.0 && camera->fov_y_radians < kPi)) return GG_ERR_INVALID_ARG;
+  if (!(camera->position[1] > 0.0)) return GG_ERR_INVALID_ARG;
+  const V3 la{camera->look_at[0], camera->look_at[1], camera->look_at[2]};
+  const V3 up{camera->up[0], camera->up[1], camera->up[2]};
+  if (!(dot3(la, la) > 0.0)) return GG_ERR_INVALID_ARG;
+  const V3 cr = cross3(la, up);
+  if (!(dot3(cr, cr) > 0.0)) return GG_ERR_INVALID_ARG;  // up parallel to look_at
+  if (disk && disk->kind != GG_DISK_NONE) {
+    if (disk->kind != GG_DISK_VOLUMETRIC && disk->kind != GG_DISK_THIN) return GG_ERR_INVALID_ARG;
+    if (!(disk->r_inner > 0.0 && disk->r_outer >= disk->r_inner && std::isfinite(disk->r_outer)))
+      return GG_ERR_INVALID_ARG;
+    if (disk->kind == GG_DISK_VOLUMETRIC &&
+        !(disk->scale_height > 0.0 && std::isfinite(disk->scale_height) &&
+          std::isfinite(disk->density_0) && std::isfinite(disk->temperature_0)))
+      return GG_ERR_INVALID_ARG;
+    if (disk->kind == GG_DISK_THIN && !std::isfinite(disk->emissivity_index))
+      return GG_ERR_INVALID_ARG;
+  }
+  if (!(integ->initial_step > 0.0 && std::isfinite(integ->initial_step))) return GG_ERR_INVALID_ARG;
+  if (!(integ->min_step > 0.0 && integ->max_step >= integ->min_step &&
+        std::isfinite(integ->max_step)))
+    return GG_ERR_INVALID_ARG;
+  if (!(integ->rtol >= 0.0 && integ->atol >= 0.0 && std::isfinite(integ->rtol) &&
+        std::isfinite(integ->atol)))
+    return GG_ERR_INVALID_ARG;
+  if (integ->rtol > 0.0) {
+    if (!(integ->atol > 0.0)) return GG_ERR_INVALID_ARG;
+  } else if (!(integ->tolerance > 0.0 && std::isfinite(integ->tolerance))) {
+    return GG_ERR_INVALID_ARG;
+  }
+  if (!(integ->max_radius > 0.0 && std::isfinite(integ->max_radius))) return GG_ERR_INVALID_ARG;
+  if (!std::isfinite(integ->horizon_buffer)) return GG_ERR_INVALID_ARG;
+  if (integ->max_steps < 1) return GG_ERR_INVALID_ARG;
+  if (integ->precision != GG_PREC_FP64 && integ->precision != GG_PREC_MIXED)
+    return GG_ERR_INVALID_ARG;
+  if (opts->sky != GG_SKY_PROCEDURAL && opts->sky != GG_SKY_CHECKER) return GG_ERR_INVALID_ARG;
+  if (opts->sky == GG_SKY_CHECKER && (opts->sky_rows < 1 || opts->sky_cols < 1))
+    return GG_ERR_INVALID_ARG;
+  if (width < 1 || height < 1) return GG_ERR_INVALID_ARG;
+  const uint64_t spa = opts->samples_per_axis < 1 ? 1 : opts->samples_per_axis;
+  if (opts->jitter_spp == 0 && (spa * width > 0xffffffffull || spa * height > 0xffffffffull))
+    return GG_ERR_INVALID_ARG;
+  const uint64_t n = (uint64_t)width * height * spp_of(*opts);
+  if (n == 0 || n > (1ull << 40)) return GG_ERR_INVALID_ARG;
+  return GG_OK;
+}
+
+double photon_orbit(double mass, double spin) {
+  return 2.0 * mass * (1.0 + std::cos((2.0 / 3.0) * std::acos(-spin / mass)));
+}
+
+void build_params(const gg_metric_t* metric, const gg_camera_t* camera, const gg_disk_t* disk,
+                  const gg_integrator_t* integ, const gg_render_opts_t* opts, uint32_t width,
+                  uint32_t height, DevParams* out) {
+  DevParams P;
+  std::memset(&P, 0, sizeof(P));
+  P.metric = metric->kind == GG_METRIC_KERR ? gg::kMetricKerr : gg::kMetricSchwarzschild;
+  P.mass = metric->mass;
+  P.spin = metric->kind == GG_METRIC_KERR ? metric->spin : 0.0;
+  P.rs = 2.0 * metric->mass;
+  if (P.metric == gg::kMetricKerr) {  // kerr.rs:427-436
+    const double disc = P.mass * P.mass - P.spin * P.spin;
+    P.has_horizon = disc < 0.0 ? 0 : 1;
+    P.rh = disc < 0.0 ? 0.0 : P.mass + std::sqrt(disc);
+    P.r_photon = photon_orbit(P.mass, P.spin);
+  } else {
+    P.has_horizon = 1;
+    P.rh = P.rs;
+    P.r_photon = 3.0 * P.mass;
+  }
+  P.rh_plus_buffer = P.rh + integ->horizon_buffer;
+  P.initial_step = integ->initial_step;
+  P.min_step = integ->min_step;
+  P.max_step = integ->max_step;
+  P.tolerance = integ->tolerance;
+  P.max_radius = integ->max_radius;
+  P.rtol = integ->rtol;
+  P.atol = integ->atol;
+  P.max_steps = integ->max_steps;
+  P.precision = integ->precision;
+
+  P.width = width;
+  P.height = height;
+  P.jitter_spp = opts->jitter_spp;
+  P.spa = opts->jitter_spp > 0 ? 1 : (opts->samples_per_axis < 1 ? 1 : opts->samples_per_axis);
+  P.spp = spp_of(*opts);
+  P.sub_w = width * P.spa;
+  P.sub_h = height * P.spa;
+  P.seed = opts->seed;
+  P.n_rays = (uint64_t)width * height * P.spp;
+  P.inv_spp = 1.0 / (double)P.spp;
+
+  // Camera::pixel_direction frame (camera.rs:20-29)
+  const V3 la{camera->look_at[0], camera->look_at[1], camera->look_at[2]};
+  const V3 upv{camera->up[0], camera->up[1], camera->up[2]};
+  const V3 forward = normalize3(la);
+  const V3 right = normalize3(cross3(forward, upv));
+  const V3 up2 = normalize3(cross3(right, forward));
+  P.cam_forward[0] = forward.x; P.cam_forward[1] = forward.y; P.cam_forward[2] = forward.z;
+  P.cam_right[0] = right.x; P.cam_right[1] = right.y; P.cam_right[2] = right.z;
+  P.cam_up[0] = up2.x; P.cam_up[1] = up2.y; P.cam_up[2] = up2.z;
+  P.half_h = std::tan(camera->fov_y_radians / 2.0);
+  P.half_w = P.half_h * camera->aspect;
+  // local spherical frame and metric at the camera (ray.rs:29-48)
+  for (int i = 0; i < 4; ++i) P.cam_pos[i] = camera->position[i];
+  const double theta = camera->position[2], phi = camera->position[3];
+  const double st = std::sin(theta), ct = std::cos(theta);
+  const double sp = std::sin(phi), cp = std::cos(phi);
+  P.r_hat[0] = st * cp; P.r_hat[1] = st * sp; P.r_hat[2] = ct;
+  P.theta_hat[0] = ct * cp; P.theta_hat[1] = ct * sp; P.theta_hat[2] = -st;
+  P.phi_hat[0] = -sp; P.phi_hat[1] = cp; P.phi_hat[2] = 0.0;
+  const G5 g = metric_at(*metric, camera->position);
+  P.cam_g_tt = g.tt;
+  P.cam_g_rr = g.rr;
+  P.cam_g_thth = g.thth;
+  P.cam_g_phph = g.phph;
+  P.sqrt_g_rr = std::sqrt(g.rr);
+  P.sqrt_g_thth = std::sqrt(g.thth);
+  P.sqrt_g_phph = std::sqrt(g.phph);
+  P.sqrt_neg_gtt_obs = std::sqrt(std::fmax(-g.tt, 0.0));  // tracer.rs:93-94
+
+  P.disk = disk ? disk->kind : GG_DISK_NONE;
+  if (disk) {
+    P.r_inner = disk->r_inner;
+    P.r_outer = disk->r_outer;
+    P.scale_height = disk->scale_height;
+    P.density_0 = disk->density_0;
+    P.temperature_0 = disk->temperature_0;
+    P.emissivity_index = disk->emissivity_index;
+  }
+  P.sky = opts->sky;
+  P.sky_rows = opts->sky_rows;
+  P.sky_cols = opts->sky_cols;
+  P.sky_seed = opts->sky_seed;
+  P.cell_h = kPi / (double)(opts->sky_rows ? opts->sky_rows : 1);
+  P.cell_w = (2.0 * kPi) / (double)(opts->sky_cols ? opts->sky_cols : 1);
+  P.attempt_budget = opts->attempt_budget;
+  *out = P;
+}
+
+int grow(void** buf, size_t* cap, size_t need) {
+  if (need <= *cap) return GG_OK;
+  if (*buf) cudaFree(*buf);
+  *buf = nullptr;
+  *cap = 0;
+  size_t want = need + need / 4;
+  if (cudaMalloc(buf, want) != cudaSuccess) {
+    cudaGetLastError();
+    if (cudaMalloc(buf, need) != cudaSuccess) {
+      cudaGetLastError();
+      *buf = nullptr;
+      return GG_ERR_OOM;
+    }
+    want = need;
+  }
+  *cap = want;
+  return GG_OK;
+}
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+// Enqueues one render with device outputs O on `stream`.
+int enqueue(gg_ctx* ctx, const DevParams& P, DevOutputs O, bool want_image,
+            cudaStream_t stream) {
+  if (cudaStreamWaitEvent(stream, ctx->ev_done, 0) != cudaSuccess) return GG_ERR_CUDA;
+  if (want_image && P.spp > 1) {
+    const int st = grow(&ctx->samples, &ctx->samples_cap, sizeof(double) * 3 * P.n_rays);
+    if (st != GG_OK) return st;
+    O.sample_rgb = static_cast<double*>(ctx->samples);
+  } else {
+    O.sample_rgb = nullptr;
+  }
+  if (!want_image) O.rgb8 = nullptr;
+  if (cudaMemsetAsync(ctx->ctl, 0, sizeof(DevControl), stream) != cudaSuccess) return GG_ERR_CUDA;
+  int bps = 0;
+  if (gg::trace_occupancy(P, &bps) != cudaSuccess || bps < 1) return GG_ERR_CUDA;
+  uint64_t grid = (uint64_t)ctx->sms * (uint64_t)bps;
+  const uint64_t need_blocks = (P.n_rays + gg::kTraceBlock - 1) / gg::kTraceBlock;
+  if (grid > need_blocks) grid = need_blocks;
+  if (grid < 1) grid = 1;
+  if (cudaEventRecord(ctx->ev_start, stream) != cudaSuccess) return GG_ERR_CUDA;
+  if (gg::launch_trace(P, O, ctx->ctl, (int)grid, stream) != cudaSuccess) return GG_ERR_CUDA;
+  if (cudaEventRecord(ctx->ev_stop, stream) != cudaSuccess) return GG_ERR_CUDA;
+  if (O.sample_rgb && O.rgb8) {
+    if (gg::launch_reduce(P, O.sample_rgb, O.rgb8, ctx->sms, stream) != cudaSuccess)
+      return GG_ERR_CUDA;
+  }
+  if (cudaMemcpyAsync(ctx->ctl_host, ctx->ctl, sizeof(DevControl), cudaMemcpyDeviceToHost,
+                      stream) != cudaSuccess)
+    return GG_ERR_CUDA;
+  if (cudaEventRecord(ctx->ev_done, stream) != cudaSuccess) return GG_ERR_CUDA;
+  ctx->pending = true;
+  return GG_OK;
+}
+
+// Waits for the last render and folds its counters into ctx->last.
+int collect(gg_ctx* ctx) {
+  if (!ctx->pending) return GG_OK;
+  if (cudaEventSynchronize(ctx->ev_done) != cudaSuccess) return GG_ERR_CUDA;
+  ctx->pending = false;
+  const DevControl& c = *ctx->ctl_host;
+  gg_stats_t s{};
+  s.attempts = c.attempts;
+  s.accepted = c.accepted;
+  for (int k = 0; k < 5; ++k) {
+    s.class_count[k] = c.class_count[k];
+    s.rays += c.class_count[k];
+  }
+  float ms = 0.f;
+  if (cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop) == cudaSuccess) s.kernel_ms = ms;
+  ctx->last = s;
+  return c.abort ? GG_ERR_BUDGET : GG_OK;
+}
+
+struct Lock {
+  explicit Lock(gg_ctx* c) : g(c->mu) { cudaSetDevice(c->device); }
+  std::lock_guard<std::mutex> g;
+};
+
+}  // namespace
+
+extern "C" {
+
+GG_API const char* gg_version(void) { return "gargantua_b200 0.1.0 (sm_100a)"; }
+
+GG_API const char* gg_strerror(int status) {
+  switch (status) {
+    case GG_OK: return "ok";
+    case GG_ERR_INVALID_ARG: return "invalid argument";
+    case GG_ERR_CUDA: return "CUDA runtime error";
+    case GG_ERR_OOM: return "device out of memory";
+    case GG_ERR_BUDGET: return "attempt budget exhausted";
+    case GG_ERR_UNSUPPORTED: return "unsupported combination";
+    case GG_ERR_NO_DEVICE: return "no sm_100 CUDA device";
+    default: return "unknown status";
+  }
+}
+
+GG_API int gg_struct_size(const char* name) {
+  if (!name) return -1;
+  struct {
+    const char* n;
+    int s;
+  } t[] = {{"gg_metric_t", (int)sizeof(gg_metric_t)},
+           {"gg_camera_t", (int)sizeof(gg_camera_t)},
+           {"gg_disk_t", (int)sizeof(gg_disk_t)},
+           {"gg_integrator_t", (int)sizeof(gg_integrator_t)},
+           {"gg_render_opts_t", (int)sizeof(gg_render_opts_t)},
+           {"gg_ray_out_t", (int)sizeof(gg_ray_out_t)},
+           {"gg_stats_t", (int)sizeof(gg_stats_t)}};
+  for (auto& e : t)
+    if (std::strcmp(e.n, name) == 0) return e.s;
+  return -1;
+}
+
+GG_API int gg_metric_schwarzschild(gg_metric_t* out, double mass) {
+  if (!out) return GG_ERR_INVALID_ARG;
+  std::memset(out, 0, sizeof(*out));
+  out->kind = GG_METRIC_SCHWARZSCHILD;
+  out->mass = mass;
+  return (std::isfinite(mass) && mass > 0.0) ? GG_OK : GG_ERR_INVALID_ARG;
+}
+
+GG_API int gg_metric_kerr(gg_metric_t* out, double mass, double spin) {
+  if (!out) return GG_ERR_INVALID_ARG;
+  std::memset(out, 0, sizeof(*out));
+  out->kind = GG_METRIC_KERR;
+  out->mass = mass;
+  if (!(std::isfinite(mass) && mass > 0.0)) return GG_ERR_INVALID_ARG;  // kerr.rs:30
+  const double max_spin = mass * 0.9999;                                  // kerr.rs:31-32
+  out->spin = spin < -max_spin ? -max_spin : (spin > max_spin ? max_spin : spin);
+  return std::isfinite(spin) ? GG_OK : GG_ERR_INVALID_ARG;
+}
+
+GG_API void gg_integrator_default(gg_integrator_t* out) {
+  if (!out) return;
+  std::memset(out, 0, sizeof(*out));
+  out->initial_step = 0.1;  // geodesic.rs:170-181
+  out->min_step = 1e-8;
+  out->max_step = 1.0;
+  out->tolerance = 1e-6;
+  out->max_radius = 200.0;  // renderer.rs:264
+  out->horizon_buffer = 0.01;
+  out->max_steps = 5000;    // renderer.rs:265
+  out->precision = GG_PREC_FP64;
+}
+
+GG_API void gg_disk_default(gg_disk_t* out) {
+  if (!out) return;
+  std::memset(out, 0, sizeof(*out));
+  out->kind = GG_DISK_VOLUMETRIC;  // disk.rs:21-31
+  out->r_inner = 6.0;
+  out->r_outer = 20.0;
+  out->scale_height = 1.0;
+  out->density_0 = 1.0;
+  out->temperature_0 = 1.0;
+  out->emissivity_index = 3.0;
+}
+
+GG_API void gg_render_opts_default(gg_render_opts_t* out) {
+  if (!out) return;
+  std::memset(out, 0, sizeof(*out));
+  out->samples_per_axis = 1;
+  out->sky = GG_SKY_PROCEDURAL;
+  out->sky_rows = 18;
+  out->sky_cols = 36;
+}
+
+GG_API int gg_camera_inclined(gg_camera_t* out, double r, double inclination_rad,
+                              double fov_y_radians, double aspect) {
+  if (!out) return GG_ERR_INVALID_ARG;
+  std::memset(out, 0, sizeof(*out));
+  out->position[0] = 0.0;
+  out->position[1] = r;
+  out->position[2] = inclination_rad;
+  out->position[3] = 0.0;
+  out->look_at[0] = -std::sin(inclination_rad);
+  out->look_at[1] = 0.0;
+  out->look_at[2] = -std::cos(inclination_rad);
+  out->up[2] = 1.0;
+  out->fov_y_radians = fov_y_radians;
+  out->aspect = aspect;
+  const bool ok = r > 0.0 && std::isfinite(r) && inclination_rad > 0.0 &&
+                  inclination_rad < kPi && fov_y_radians > 0.0 && fov_y_radians < kPi &&
+                  aspect > 0.0 && std::isfinite(aspect);
+  return ok ? GG_OK : GG_ERR_INVALID_ARG;
+}
+
+GG_API double gg_kerr_isco(double mass, double spin) {
+  // Bardeen, Press & Teukolsky (1972), prograde orbit.
+  const double a = spin / mass;
+  const double z1 = 1.0 + std::cbrt(1.0 - a * a) * (std::cbrt(1.0 + a) + std::cbrt(1.0 - a));
+  const double z2 = std::sqrt(3.0 * a * a + z1 * z1);
+  return mass * (3.0 + z2 - std::sqrt((3.0 - z1) * (3.0 + z1 + 2.0 * z2)));
+}
+
+GG_API double gg_kerr_photon_orbit(double mass, double spin) { return photon_orbit(mass, spin); }
+
+GG_API int gg_validate(const gg_metric_t* metric, const gg_camera_t* camera,
+                       const gg_disk_t* disk, const gg_integrator_t* integ,
+                       const gg_render_opts_t* opts, uint32_t width, uint32_t height) {
+  return validate(metric, camera, disk, integ, opts, width, height);
+}
+
+GG_API int gg_create(gg_ctx** out, int device) {
+  if (!out) return GG_ERR_INVALID_ARG;
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count <= 0) {
+    cudaGetLastError();
+    return GG_ERR_NO_DEVICE;
+  }
+  if (device < 0 || device >= count) return GG_ERR_INVALID_ARG;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return GG_ERR_CUDA;
+  if (prop.major != 10) return GG_ERR_NO_DEVICE;  // built for sm_100a only
+  if (cudaSetDevice(device) != cudaSuccess) return GG_ERR_CUDA;
+  gg_ctx* c = new (std::nothrow) gg_ctx();
+  if (!c) return GG_ERR_OOM;
+  c->device = device;
+  c->sms = prop.multiProcessorCount;
+  bool ok = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaEventCreate(&c->ev_start) == cudaSuccess &&
+            cudaEventCreate(&c->ev_stop) == cudaSuccess &&
+            cudaEventCreateWithFlags(&c->ev_done, cudaEventDisableTiming) == cudaSuccess &&
+            cudaMalloc(&c->ctl, sizeof(DevControl)) == cudaSuccess &&
+            cudaMallocHost(&c->ctl_host, sizeof(DevControl)) == cudaSuccess;
+  if (!ok) {
+    gg_destroy(c);
+    return GG_ERR_CUDA;
+  }
+  std::memset(c->ctl_host, 0, sizeof(DevControl));
+  cudaEventRecord(c->ev_done, c->stream);
+  *out = c;
+  return GG_OK;
+}
+
+GG_API int gg_destroy(gg_ctx* c) {
+  if (!c) return GG_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->pending && c->ev_done) cudaEventSynchronize(c->ev_done);
+  if (c->samples) cudaFree(c->samples);
+  if (c->staging) cudaFree(c->staging);
+  if (c->ctl) cudaFree(c->ctl);
+  if (c->ctl_host) cudaFreeHost(c->ctl_host);
+  if (c->ev_start) cudaEventDestroy(c->ev_start);
+  if (c->ev_stop) cudaEventDestroy(c->ev_stop);
+  if (c->ev_done) cudaEventDestroy(c->ev_done);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return GG_OK;
+}
+
+GG_API void* gg_stream(gg_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+GG_API int gg_last_stats(gg_ctx* c, gg_stats_t* out) {
+  if (!c || !out) return GG_ERR_INVALID_ARG;
+  Lock lock(c);
+  const int st = collect(c);
+  *out = c->last;
+  return st == GG_ERR_BUDGET ? GG_OK : st;
+}
+
+GG_API int gg_render_device(gg_ctx* c, const gg_metric_t* metric, const gg_camera_t* camera,
+                            const gg_disk_t* disk, const gg_integrator_t* integ,
+                            const gg_render_opts_t* opts, uint32_t width, uint32_t height,
+                            uint8_t* rgb_dev, const gg_ray_out_t* rays_dev, void* stream) {
+  if (!c) return GG_ERR_INVALID_ARG;
+  const int v = validate(metric, camera, disk, integ, opts, width, height);
+  if (v != GG_OK) return v;
+  if (integ->precision != GG_PREC_FP64) return GG_ERR_UNSUPPORTED;
+  DevParams P;
+  build_params(metric, camera, disk, integ, opts, width, height, &P);
+  Lock lock(c);
+  DevOutputs O;
+  std::memset(&O, 0, sizeof(O));
+  if (rays_dev) {
+    O.cls = rays_dev->cls;
+    O.x = rays_dev->x;
+    O.v = rays_dev->v;
+    O.lam = rays_dev->lambda;
+    O.attempts = rays_dev->attempts;
+    O.accepted = rays_dev->accepted;
+    O.intensity = rays_dev->intensity;
+    O.color_temp = rays_dev->color_temp;
+    O.rgb = rays_dev->rgb;
+    O.cross = rays_dev->cross;
+  }
+  O.rgb8 = rgb_dev;
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+  return enqueue(c, P, O, rgb_dev != nullptr, s);
+}
+
+GG_API int gg_render(gg_ctx* c, const gg_metric_t* metric, const gg_camera_t* camera,
+                     const gg_disk_t* disk, const gg_integrator_t* integ,
+                     const gg_render_opts_t* opts, uint32_t width, uint32_t height,
+                     uint8_t* rgb_out, const gg_ray_out_t* rays_out) {
+  if (!c) return GG_ERR_INVALID_ARG;
+  const int v = validate(metric, camera, disk, integ, opts, width, height);
+  if (v != GG_OK) return v;
+  if (integ->precision != GG_PREC_FP64) return GG_ERR_UNSUPPORTED;
+  DevParams P;
+  build_params(metric, camera, disk, integ, opts, width, height, &P);
+  Lock lock(c);
+  const uint64_t n = P.n_rays;
+  const size_t n_pix = (size_t)width * height;
+
+  // lay out the device staging buffer for every requested output
+  struct Slot {
+    void* host;
+    size_t bytes;
+    size_t off;
+  };
+  Slot slots[11];
+  int ns = 0;
+  size_t total = 0;
+  auto add = [&](void* host, size_t bytes) -> size_t {
+    if (!host) return (size_t)-1;
+    slots[ns] = {host, bytes, total};
+    ++ns;
+    const size_t off = total;
+    total += align256(bytes);
+    return off;
+  };
+  const size_t o_rgb8 = add(rgb_out, n_pix * 3);
+  size_t o_arr[10];
+  for (int k = 0; k < 10; ++k) o_arr[k] = (size_t)-1;
+  if (rays_out) {
+    o_arr[0] = add(rays_out->cls, n * sizeof(int32_t));
+    o_arr[1] = add(rays_out->x, n * 4 * sizeof(double));
+    o_arr[2] = add(rays_out->v, n * 4 * sizeof(double));
+    o_arr[3] = add(rays_out->lambda, n * sizeof(double));
+    o_arr[4] = add(rays_out->attempts, n * sizeof(uint32_t));
+    o_arr[5] = add(rays_out->accepted, n * sizeof(uint32_t));
+    o_arr[6] = add(rays_out->intensity, n * sizeof(double));
+    o_arr[7] = add(rays_out->color_temp, n * sizeof(double));
+    o_arr[8] = add(rays_out->rgb, n * 3 * sizeof(double));
+    o_arr[9] = add(rays_out->cross, n * 8 * sizeof(double));
+  }
+  if (total > 0) {
+    const int st = grow(&c->staging, &c->staging_cap, total);
+    if (st != GG_OK) return st;
+  }
+  char* base = static_cast<char*>(c->staging);
+  auto dp = [&](size_t off) -> void* { return off == (size_t)-1 ? nullptr : base + off; };
+  DevOutputs O;
+  std::memset(&O, 0, sizeof(O));
+  O.rgb8 = static_cast<uint8_t*>(dp(o_rgb8));
+  O.cls = static_cast<int32_t*>(dp(o_arr[0]));
+  O.x = static_cast<double*>(dp(o_arr[1]));
+  O.v = static_cast<double*>(dp(o_arr[2]));
+  O.lam = static_cast<double*>(dp(o_arr[3]));
+  O.attempts = static_cast<uint32_t*>(dp(o_arr[4]));
+  O.accepted = static_cast<uint32_t*>(dp(o_arr[5]));
+  O.intensity = static_cast<double*>(dp(o_arr[6]));
+  O.color_temp = static_cast<double*>(dp(o_arr[7]));
+  O.rgb = static_cast<double*>(dp(o_arr[8]));
+  O.cross = static_cast<double*>(dp(o_arr[9]));
+
+  int st = enqueue(c, P, O, rgb_out != nullptr, c->stream);
+  if (st != GG_OK) return st;
+  for (int k = 0; k < ns; ++k) {
+    if (cudaMemcpyAsync(slots[k].host, base + slots[k].off, slots[k].bytes,
+                        cudaMemcpyDeviceToHost, c->stream) != cudaSuccess)
+      return GG_ERR_CUDA;
+  }
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return GG_ERR_CUDA;
+  return collect(c);
+}
+
+}  // extern "C"

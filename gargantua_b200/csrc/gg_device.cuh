@@ -1,0 +1,495 @@
+// gg_device.cuh -- device-side physics of the GR ray path for sm_100a.
+//
+// One CUDA thread carries one geodesic through gargantua's RK45 stepper
+// (crates/gr-core/src/geodesic.rs:185-328).  The ray state lives in
+// registers for the whole trace; only the finished outcome goes to HBM.
+//
+// Formulation vs the reference.  The reference evaluates Kerr's right-hand
+// side by filling a dense 4x4x4 Christoffel array from ~15 divisions and
+// contracting all 64 entries (crates/gr-core/src/metric.rs:37-52,
+// crates/gr-core/src/kerr.rs:100-424).  Here the same 20 non-zero symbols are
+// folded into the contraction: the t and phi rows share the two "energy"
+// sums E_t, E_phi, the r and theta rows share their g^rr, g^thth factor, and
+// all of 1/Sigma, 1/Delta, 1/sin^2 come from one reciprocal.  The result is
+// the same function of (x, v) to rounding.  The stepper's control flow
+// (termination tests at the start of a step, invalid-stage halving, the
+// acceptance test and the step-size law) is the reference's, test for test.
+#pragma once
+
+#include <cstdint>
+
+#include "gg_params.h"
+
+namespace gg {
+
+#define GG_DEV __device__ __forceinline__
+
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kHalfPi = kPi / 2.0;
+constexpr double kTwoPi = 2.0 * kPi;
+
+// Non-contracted double arithmetic, for the few places that must reproduce
+// the reference's rounding bit for bit (ray setup, shading, encoding).
+GG_DEV double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+GG_DEV double add_rn(double a, double b) { return __dadd_rn(a, b); }
+GG_DEV double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+
+// ---------------------------------------------------------------------------
+// Geodesic right-hand side a^mu = -Gamma^mu_ab v^a v^b.
+// ---------------------------------------------------------------------------
+
+// Schwarzschild (schwarzschild.rs:99-140), one reciprocal.
+GG_DEV void rhs_schwarzschild(const DevParams& P, double r_in, double th, const double v[4],
+                              double a[4]) {
+  const double r = fmax(r_in, 1e-10);
+  double s, c;
+  sincos(th, &s, &c);
+  const double rs = P.rs;
+  const double rmrs = r - rs;
+  const double R = 1.0 / (r * rmrs * s);  // 1 / (r (r - rs) sin)
+  const double ifd = s * R;                // 1 / (r (r - rs))
+  const double ir = rmrs * ifd;            // 1 / r
+  const double is = (r * rmrs) * R;        // 1 / sin
+  const double g_t_tr = 0.5 * rs * ifd;
+  const double g_r_tt = 0.5 * rs * rmrs * (ir * ir * ir);
+  const double g_r_thth = -rmrs;
+  const double g_r_phph = -rmrs * s * s;
+  const double g_th_phph = -s * c;
+  const double g_ph_thph = c * is;
+  const double vt = v[0], vr = v[1], vth = v[2], vph = v[3];
+  a[0] = -2.0 * g_t_tr * vt * vr;
+  a[1] = -g_r_tt * vt * vt + g_t_tr * vr * vr - g_r_thth * vth * vth - g_r_phph * vph * vph;
+  a[2] = -2.0 * ir * vr * vth - g_th_phph * vph * vph;
+  a[3] = -2.0 * ir * vr * vph - 2.0 * g_ph_thph * vth * vph;
+}
+
+// Kerr in Boyer-Lindquist coordinates.  Metric derivatives are the
+// reference's (kerr.rs:154-204) with shared factors pulled out; the
+// contraction groups the symbols by row as described at the top.
+template <class T>
+GG_DEV void rhs_kerr_t(T M, T a, T r_in, T s, T c, const T v[4], T acc[4]) {
+  const T r = r_in;
+  const T r2 = r * r, a2 = a * a, s2 = s * s, c2 = c * c, sc = s * c;
+  const T sig = r2 + a2 * c2;
+  const T del = (r - T(2) * M) * r + a2;
+  const T rho = r2 + a2;
+  const T sd = sig * del;
+  const T R = T(1) / (sd * s2);
+  const T iSD = s2 * R;        // 1 / (Sigma Delta)
+  const T iS = del * iSD;      // 1 / Sigma
+  const T iD = sig * iSD;      // 1 / Delta
+  const T is2 = sd * R;        // 1 / sin^2
+  const T iS2 = iS * iS;
+  const T Mr = M * r;
+  // d_r and d_theta of g_tt, g_rr, g_thth, g_phph, g_tphi
+  const T sm2r = a2 * c2 - r2;  // Sigma - 2 r^2
+  const T dtt_r = T(2) * M * sm2r * iS2;
+  const T dtt_th = T(4) * Mr * a2 * sc * iS2;
+  const T drr_r = T(2) * (a2 * (r * s2 + M * c2) - M * r2) * (iD * iD);
+  const T drr_th = T(-2) * a2 * sc * iD;
+  const T dthth_r = T(2) * r;
+  const T dthth_th = T(-2) * a2 * sc;
+  const T dphph_r = T(2) * r * s2 + T(2) * M * a2 * (s2 * s2) * sm2r * iS2;
+  const T dphph_th = T(2) * rho * sc + T(2) * Mr * a2 * sc * s2 * (T(2) * (sig + rho)) * iS2;
+  const T dtph_r = T(-2) * M * a * s2 * sm2r * iS2;
+  const T dtph_th = T(-4) * Mr * a * sc * rho * iS2;
+  // inverse metric
+  const T big_a = rho * rho - a2 * del * s2;
+  const T gtt = -big_a * iSD;
+  const T gtph = T(-2) * Mr * a * iSD;
+  const T grr = del * iS;
+  const T gthth = iS;
+  const T gphph = (del - a2 * s2) * iSD * is2;
+  const T vt = v[0], vr = v[1], vth = v[2], vph = v[3];
+  const T Et = vr * (dtt_r * vt + dtph_r * vph) + vth * (dtt_th * vt + dtph_th * vph);
+  const T Ep = vr * (dtph_r * vt + dphph_r * vph) + vth * (dtph_th * vt + dphph_th * vph);
+  acc[0] = -(gtt * Et + gtph * Ep);
+  acc[3] = -(gtph * Et + gphph * Ep);
+  const T vt2 = vt * vt, vr2 = vr * vr, vth2 = vth * vth, vph2 = vph * vph;
+  const T two_tp = T(2) * vt * vph, two_rt = T(2) * vr * vth;
+  acc[1] = T(-0.5) * grr *
+           (drr_r * vr2 - dtt_r * vt2 - dthth_r * vth2 - dphph_r * vph2 + drr_th * two_rt -
+            dtph_r * two_tp);
+  acc[2] = T(-0.5) * gthth *
+           (dthth_th * vth2 - dtt_th * vt2 - drr_th * vr2 - dphph_th * vph2 +
+            dthth_r * two_rt - dtph_th * two_tp);
+}
+
+GG_DEV void rhs_kerr(const DevParams& P, double r_in, double th, const double v[4],
+                     double a[4]) {
+  double s, c;
+  sincos(th, &s, &c);
+  rhs_kerr_t<double>(P.mass, P.spin, fmax(r_in, 1e-10), s, c, v, a);
+}
+
+template <int METRIC>
+GG_DEV void rhs(const DevParams& P, double r, double th, const double v[4], double a[4]) {
+  if (METRIC == kMetricKerr) {
+    rhs_kerr(P, r, th, v, a);
+  } else {
+    rhs_schwarzschild(P, r, th, v, a);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Metric components and the redshift of a Keplerian emitter (used per
+// accepted step by the disks, not per stage).
+// ---------------------------------------------------------------------------
+struct Gmet {
+  double tt, rr, thth, phph, tph;
+};
+
+template <int METRIC>
+GG_DEV Gmet metric_tensor(const DevParams& P, double r_in, double th) {
+  const double r = fmax(r_in, 1e-10);
+  const double s = sin(th);
+  Gmet g;
+  if (METRIC == kMetricKerr) {  // kerr.rs:61-94
+    const double m = P.mass, a = P.spin, a2 = a * a;
+    const double c = cos(th);
+    const double sig = r * r + a * a * c * c;
+    const double del = r * r - 2.0 * m * r + a * a;
+    const double sin2 = s * s;
+    g.tt = -(1.0 - 2.0 * m * r / sig);
+    g.rr = sig / del;
+    g.thth = sig;
+    g.phph = (r * r + a2 + 2.0 * m * a2 * r * sin2 / sig) * sin2;
+    g.tph = -2.0 * m * a * r * sin2 / sig;
+  } else {  // schwarzschild.rs:26-43
+    const double f = 1.0 - P.rs / r;
+    g.tt = -f;
+    g.rr = 1.0 / f;
+    g.thth = r * r;
+    g.phph = r * r * s * s;
+    g.tph = 0.0;
+  }
+  return g;
+}
+
+// redshift_factor (crates/raytracer/src/curved/tracer.rs:158-183) with the
+// metric's orbital_four_velocity (schwarzschild.rs:146-153, kerr.rs:439-449)
+// and circular_orbit_velocity (metric.rs:82-94).
+template <int METRIC>
+GG_DEV double redshift_factor(const DevParams& P, double r, double th, const double p[4]) {
+  const Gmet g = metric_tensor<METRIC>(P, r, th);
+  const double p_t = g.tt * p[0] + g.tph * p[3];
+  const double e_obs = fmax(-p_t / P.sqrt_neg_gtt_obs, 0.0);
+  bool has_orbit;
+  double omega = 0.0;
+  if (METRIC == kMetricKerr) {
+    has_orbit = r > 0.0;
+    if (has_orbit) {
+      const double sqrt_m = sqrt(P.mass);
+      omega = sqrt_m / (pow(r, 1.5) + P.spin * sqrt_m);
+    }
+  } else {
+    has_orbit = !(r <= 3.0 * P.mass);
+    if (has_orbit) omega = sqrt(P.mass / (r * r * r));
+  }
+  double e_emit = 0.0;
+  bool used_orbit = false;
+  if (has_orbit) {
+    const Gmet go = metric_tensor<METRIC>(P, r, th);
+    const double denom = -(go.tt + 2.0 * go.tph * omega + go.phph * omega * omega);
+    if (denom > 0.0 && isfinite(denom)) {
+      const double u_t = 1.0 / sqrt(denom);
+      const double u_p = omega * u_t;
+      const double p_phi = g.tph * p[0] + g.phph * p[3];
+      e_emit = fmax(-(p_t * u_t + p_phi * u_p), 0.0);
+      used_orbit = true;
+    }
+  }
+  if (!used_orbit) {
+    const double g_tt_emit = -g.tt;
+    e_emit = fmax(g_tt_emit > 0.0 ? -p_t / sqrt(g_tt_emit) : 0.0, 0.0);
+  }
+  return e_emit > 0.0 ? e_obs / e_emit : 0.0;
+}
+
+// ---------------------------------------------------------------------------
+// Ray state and one RK45 attempt.
+// ---------------------------------------------------------------------------
+struct Ray {
+  double x[4];
+  double v[4];
+  double h;
+  double lam;
+};
+
+enum StepResult { kContinue = 0, kHorizon = 1, kEscaped = 2 };
+
+GG_DEV bool finite4(double a, double b, double c, double d) {
+  return isfinite(a) && isfinite(b) && isfinite(c) && isfinite(d);
+}
+
+// normalize_spherical_coords (geodesic.rs:337-352)
+GG_DEV void normalize_coords(double x[4]) {
+  if (x[2] < 0.0) {
+    x[2] = -x[2];
+    x[3] = x[3] + kPi;
+  }
+  if (x[2] > kPi) {
+    x[2] = kTwoPi - x[2];
+    x[3] = x[3] + kPi;
+  }
+  double m = fmod(x[3], kTwoPi);
+  if (m < 0.0) m = m + kTwoPi;
+  x[3] = m;
+}
+
+// Dormand-Prince tableau (geodesic.rs:210-242).
+struct DP {
+  static constexpr double a2 = 1.0 / 5.0, a3 = 3.0 / 10.0, a4 = 4.0 / 5.0, a5 = 8.0 / 9.0;
+  static constexpr double b21 = 1.0 / 5.0;
+  static constexpr double b31 = 3.0 / 40.0, b32 = 9.0 / 40.0;
+  static constexpr double b41 = 44.0 / 45.0, b42 = -56.0 / 15.0, b43 = 32.0 / 9.0;
+  static constexpr double b51 = 19372.0 / 6561.0, b52 = -25360.0 / 2187.0,
+                          b53 = 64448.0 / 6561.0, b54 = -212.0 / 729.0;
+  static constexpr double b61 = 9017.0 / 3168.0, b62 = -355.0 / 33.0, b63 = 46732.0 / 5247.0,
+                          b64 = 49.0 / 176.0, b65 = -5103.0 / 18656.0;
+  static constexpr double c1 = 35.0 / 384.0, c3 = 500.0 / 1113.0, c4 = 125.0 / 192.0,
+                          c5 = -2187.0 / 6784.0, c6 = 11.0 / 84.0;
+  static constexpr double d1 = 5179.0 / 57600.0, d3 = 7571.0 / 16695.0, d4 = 393.0 / 640.0,
+                          d5 = -92097.0 / 339200.0, d6 = 187.0 / 2100.0, d7 = 1.0 / 40.0;
+};
+
+// Stage position pos + (h a_i) vel (the reference moves stage positions
+// along the step's initial velocity, geodesic.rs:248-284); returns false
+// when the reference's is_valid_position would reject it.
+GG_DEV bool stage_pos(const Ray& R, double ha, double& r, double& th) {
+  const double t = R.x[0] + ha * R.v[0];
+  r = R.x[1] + ha * R.v[1];
+  th = R.x[2] + ha * R.v[2];
+  const double ph = R.x[3] + ha * R.v[3];
+  return finite4(t, r, th, ph) && r > 0.0;
+}
+
+// One call of RK45Integrator::step (geodesic.rs:185-328) in FP64.
+// Returns the StepResult; `accepted` and `h_used` describe an advance.
+template <int METRIC>
+GG_DEV int attempt_fp64(const DevParams& P, Ray& R, bool& accepted, double& h_used) {
+  accepted = false;
+  if (R.x[1] > P.max_radius) return kEscaped;
+  if (P.has_horizon && (R.x[1] < P.rh_plus_buffer || R.x[1] < P.rh)) return kHorizon;
+
+  const double h = R.h;
+  double k1[4], k2[4], k3[4], k4[4], k5[4], k6[4], k7[4], w[4];
+  double r, th;
+  rhs<METRIC>(P, R.x[1], R.x[2], R.v, k1);
+
+  if (!stage_pos(R, h * DP::a2, r, th)) { R.h = h * 0.5; return kContinue; }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) w[i] = R.v[i] + (h * DP::b21) * k1[i];
+  rhs<METRIC>(P, r, th, w, k2);
+
+  if (!stage_pos(R, h * DP::a3, r, th)) { R.h = h * 0.5; return kContinue; }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) w[i] = R.v[i] + h * (DP::b31 * k1[i] + DP::b32 * k2[i]);
+  rhs<METRIC>(P, r, th, w, k3);
+
+  if (!stage_pos(R, h * DP::a4, r, th)) { R.h = h * 0.5; return kContinue; }
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+    w[i] = R.v[i] + h * (DP::b41 * k1[i] + DP::b42 * k2[i] + DP::b43 * k3[i]);
+  rhs<METRIC>(P, r, th, w, k4);
+
+  if (!stage_pos(R, h * DP::a5, r, th)) { R.h = h * 0.5; return kContinue; }
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+    w[i] = R.v[i] +
+           h * (DP::b51 * k1[i] + DP::b52 * k2[i] + DP::b53 * k3[i] + DP::b54 * k4[i]);
+  rhs<METRIC>(P, r, th, w, k5);
+
+  if (!stage_pos(R, h, r, th)) { R.h = h * 0.5; return kContinue; }
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+    w[i] = R.v[i] + h * (DP::b61 * k1[i] + DP::b62 * k2[i] + DP::b63 * k3[i] +
+                         DP::b64 * k4[i] + DP::b65 * k5[i]);
+  rhs<METRIC>(P, r, th, w, k6);
+
+  double nv[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+    nv[i] = R.v[i] + h * (DP::c1 * k1[i] + DP::c3 * k3[i] + DP::c4 * k4[i] + DP::c5 * k5[i] +
+                          DP::c6 * k6[i]);
+  rhs<METRIC>(P, r, th, nv, k7);
+
+  double err, tol;
+  if (P.rtol > 0.0) {
+    double ssum = 0.0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const double ve = R.v[i] + h * (DP::d1 * k1[i] + DP::d3 * k3[i] + DP::d4 * k4[i] +
+                                      DP::d5 * k5[i] + DP::d6 * k6[i] + DP::d7 * k7[i]);
+      const double sc = P.atol + P.rtol * fmax(fabs(R.v[i]), fabs(nv[i]));
+      const double q = (nv[i] - ve) / sc;
+      ssum = ssum + q * q;
+    }
+    err = sqrt(ssum * 0.25);
+    tol = 1.0;
+  } else {
+    double ssum = 0.0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const double ve = R.v[i] + h * (DP::d1 * k1[i] + DP::d3 * k3[i] + DP::d4 * k4[i] +
+                                      DP::d5 * k5[i] + DP::d6 * k6[i] + DP::d7 * k7[i]);
+      const double d = nv[i] - ve;
+      ssum = ssum + d * d;
+    }
+    err = sqrt(ssum);
+    tol = P.tolerance;
+  }
+
+  if (err < tol || h <= P.min_step) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) R.x[i] = R.x[i] + h * R.v[i];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) R.v[i] = nv[i];
+    R.lam = R.lam + h;
+    normalize_coords(R.x);
+    accepted = true;
+    h_used = h;
+    if (err > 0.0) {
+      double hn = h * 0.9 * pow(tol / err, 0.2);
+      hn = hn < P.min_step ? P.min_step : (hn > P.max_step ? P.max_step : hn);
+      R.h = hn;
+    }
+  } else {
+    R.h = fmax(h * 0.9 * pow(tol / err, 0.25), P.min_step);
+  }
+  return kContinue;
+}
+
+// ---------------------------------------------------------------------------
+// Camera rays (crates/raytracer/src/curved/{camera,ray}.rs) with the
+// reference's rounding: the camera frame is prepared on the host; here only
+// the per-pixel part runs, every operation uncontracted.
+// ---------------------------------------------------------------------------
+GG_DEV uint64_t splitmix64(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ULL;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBULL;
+  return x ^ (x >> 31);
+}
+
+GG_DEV double jitter_unit(uint64_t seed, uint64_t key) {
+  return (double)(splitmix64(seed ^ splitmix64(key)) >> 11) * (1.0 / 9007199254740992.0);
+}
+
+// Image-plane (u, v) of global sample `idx` (pixel-major, samples inside).
+GG_DEV void sample_uv(const DevParams& P, uint64_t idx, double& u, double& v) {
+  const uint64_t pix = idx / P.spp;
+  const uint32_t s = (uint32_t)(idx - pix * P.spp);
+  const uint32_t py = (uint32_t)(pix / P.width);
+  const uint32_t px = (uint32_t)(pix - (uint64_t)py * P.width);
+  if (P.jitter_spp > 0) {
+    const double ox = jitter_unit(P.seed, 2 * idx);
+    const double oy = jitter_unit(P.seed, 2 * idx + 1);
+    u = sub_rn(mul_rn(__ddiv_rn(add_rn((double)px, ox), (double)P.width), 2.0), 1.0);
+    v = sub_rn(1.0, mul_rn(__ddiv_rn(add_rn((double)py, oy), (double)P.height), 2.0));
+    return;
+  }
+  const uint32_t sy = s / P.spa, sx = s - sy * P.spa;
+  const uint32_t spx = px * P.spa + sx, spy = py * P.spa + sy;
+  u = sub_rn(mul_rn(__ddiv_rn((double)spx + 0.5, (double)P.sub_w), 2.0), 1.0);
+  v = sub_rn(1.0, mul_rn(__ddiv_rn((double)spy + 0.5, (double)P.sub_h), 2.0));
+}
+
+GG_DEV double dot3_rn(const double a[3], const double b[3]) {
+  return add_rn(add_rn(mul_rn(a[0], b[0]), mul_rn(a[1], b[1])), mul_rn(a[2], b[2]));
+}
+
+// GeodesicRay::from_camera (ray.rs:14-61) for image-plane point (u, v).
+GG_DEV void init_ray(const DevParams& P, double u, double v, Ray& R) {
+  double d[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+    d[i] = add_rn(add_rn(P.cam_forward[i], mul_rn(mul_rn(u, P.half_w), P.cam_right[i])),
+                  mul_rn(mul_rn(v, P.half_h), P.cam_up[i]));
+  const double n = __dsqrt_rn(dot3_rn(d, d));
+  double dir[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) dir[i] = __ddiv_rn(d[i], n);
+  const double n_r = dot3_rn(dir, P.r_hat);
+  const double n_t = dot3_rn(dir, P.theta_hat);
+  const double n_p = dot3_rn(dir, P.phi_hat);
+  const double kr = __ddiv_rn(n_r, P.sqrt_g_rr);
+  const double kth = __ddiv_rn(n_t, P.sqrt_g_thth);
+  const double kph = __ddiv_rn(n_p, P.sqrt_g_phph);
+  const double sns = add_rn(add_rn(mul_rn(mul_rn(P.cam_g_rr, kr), kr),
+                                   mul_rn(mul_rn(P.cam_g_thth, kth), kth)),
+                            mul_rn(mul_rn(P.cam_g_phph, kph), kph));
+  const double kt = __dsqrt_rn(__ddiv_rn(-sns, P.cam_g_tt));
+#pragma unroll
+  for (int i = 0; i < 4; ++i) R.x[i] = P.cam_pos[i];
+  R.v[0] = kt;
+  R.v[1] = kr;
+  R.v[2] = kth;
+  R.v[3] = kph;
+  R.lam = 0.0;
+  R.h = P.initial_step;
+}
+
+// ---------------------------------------------------------------------------
+// Shading (crates/raytracer/src/curved/renderer.rs:44-80, sky.rs:26-40).
+// ---------------------------------------------------------------------------
+GG_DEV void procedural_sky(const double v[4], double rgb[3]) {
+  // spatial_dir (tracer.rs:185-189)
+  const double sx = v[1], sy = v[2], sz = v[3];
+  const double n = __dsqrt_rn(add_rn(add_rn(mul_rn(sx, sx), mul_rn(sy, sy)), mul_rn(sz, sz)));
+  double d0 = 1.0, d1 = 0.0, d2 = 0.0;
+  if (n > 0.0) {
+    d0 = __ddiv_rn(sx, n);
+    d1 = __ddiv_rn(sy, n);
+    d2 = __ddiv_rn(sz, n);
+  }
+  auto hash = [](double x) -> uint64_t {
+    return (uint64_t)__double_as_longlong(x) * 6364136223846793005ULL +
+           1442695040888963407ULL;
+  };
+  auto rotl = [](uint64_t x, int k) -> uint64_t { return (x << k) | (x >> (64 - k)); };
+  const uint64_t h = hash(d0) ^ rotl(hash(d1), 17) ^ rotl(hash(d2), 34);
+  if (h % 512 < 3) {
+    const double b = (double)(180u + (uint32_t)(h % 75)) / 255.0;
+    rgb[0] = rgb[1] = rgb[2] = b;
+  } else {
+    const double vv = __ddiv_rn(mul_rn(fabs(d2), 15.0), 255.0);
+    rgb[0] = 0.0;
+    rgb[1] = 0.0;
+    rgb[2] = add_rn(10.0 / 255.0, vv);
+  }
+}
+
+// Seeded checkerboard over the escape point's (theta, phi).
+GG_DEV void checker_sky(const DevParams& P, double theta, double phi, double rgb[3]) {
+  const double fi = floor(__ddiv_rn(theta, P.cell_h));
+  const double fj = floor(__ddiv_rn(phi, P.cell_w));
+  const int64_t i = fi < 0.0 ? 0 : (fi > (double)(P.sky_rows - 1) ? (int64_t)P.sky_rows - 1 : (int64_t)fi);
+  const int64_t j = fj < 0.0 ? 0 : (fj > (double)(P.sky_cols - 1) ? (int64_t)P.sky_cols - 1 : (int64_t)fj);
+  const uint64_t z = splitmix64(P.sky_seed ^ splitmix64((uint64_t)i * P.sky_cols + (uint64_t)j));
+  const double base = ((i + j) & 1) ? 0.9 : 0.1;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const double uk = (double)((z >> (21 * k)) & 0x1FFFFFULL) * (1.0 / 2097152.0);
+    rgb[k] = mul_rn(base, add_rn(0.75, mul_rn(0.25, uk)));
+  }
+}
+
+GG_DEV void disk_color(double intensity, double rgb[3]) {  // renderer.rs:62-66
+  const double x = __ddiv_rn(intensity, add_rn(1.0, intensity));
+  rgb[0] = pow(x, 0.5);
+  rgb[1] = pow(x, 1.2);
+  rgb[2] = pow(x, 2.5);
+}
+
+GG_DEV uint8_t encode_channel(double c) {  // renderer.rs:69-80
+  c = c < 0.0 ? 0.0 : (c > 1.0 ? 1.0 : c);
+  const double s = c <= 0.0031308 ? mul_rn(12.92, c)
+                                  : sub_rn(mul_rn(1.055, pow(c, 1.0 / 2.4)), 0.055);
+  const double q = round(mul_rn(s, 255.0));
+  if (!(q > 0.0)) return 0;
+  if (q > 255.0) return 255;
+  return (uint8_t)q;
+}
+
+}  // namespace gg

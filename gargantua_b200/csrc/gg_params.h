@@ -1,0 +1,87 @@
+// gg_params.h -- the launch-time parameter block of the trace kernels.
+//
+// Built once per render on the host from the public POD structs.  Every
+// per-render constant that the reference recomputes per ray (the camera's
+// orthonormal frame, tan(fov/2), the metric at the camera, the observer's
+// -g_tt) is evaluated here on the host in the reference's operation order,
+// so the kernels only do per-sample arithmetic.  Passed by value as a
+// __grid_constant__ kernel parameter (uniform across the grid).
+#pragma once
+
+#include <cstdint>
+
+namespace gg {
+
+enum : int { kMetricSchwarzschild = 0, kMetricKerr = 1 };
+enum : int { kDiskNone = 0, kDiskVolumetric = 1, kDiskThin = 2 };
+enum : int { kSkyProcedural = 0, kSkyChecker = 1 };
+enum : int { kClsHorizon = 0, kClsEscaped = 1, kClsDisk = 2, kClsMaxSteps = 3, kClsBudget = 4 };
+
+struct DevParams {
+  // metric
+  int metric;
+  int has_horizon;
+  double mass, spin, rs;
+  double rh, rh_plus_buffer;
+  double r_photon;  // prograde circular photon orbit (mixed form's FP64 band)
+  // integrator
+  double initial_step, min_step, max_step, tolerance, max_radius;
+  double rtol, atol;
+  uint32_t max_steps;
+  int precision;
+  // sampling
+  uint32_t width, height, spa, spp, jitter_spp, sub_w, sub_h;
+  uint32_t pad0;
+  uint64_t seed;
+  uint64_t n_rays;
+  // camera frame (camera.rs:20-29, ray.rs:29-48), host-evaluated
+  double cam_pos[4];
+  double cam_forward[3], cam_right[3], cam_up[3];
+  double half_w, half_h;
+  double r_hat[3], theta_hat[3], phi_hat[3];
+  double cam_g_tt, cam_g_rr, cam_g_thth, cam_g_phph;
+  double sqrt_g_rr, sqrt_g_thth, sqrt_g_phph;
+  double sqrt_neg_gtt_obs;  // tracer.rs:93-94
+  // disk
+  int disk;
+  int pad1;
+  double r_inner, r_outer, scale_height, density_0, temperature_0, emissivity_index;
+  // sky
+  int sky;
+  uint32_t sky_rows, sky_cols;
+  uint32_t pad2;
+  uint64_t sky_seed;
+  double cell_h, cell_w;
+  // control
+  uint64_t attempt_budget;
+  double inv_spp;
+};
+
+// Device pointers of one render's outputs (each nullable).
+struct DevOutputs {
+  int32_t* cls;
+  double* x;
+  double* v;
+  double* lam;
+  uint32_t* attempts;
+  uint32_t* accepted;
+  double* intensity;
+  double* color_temp;
+  double* rgb;
+  double* cross;
+  uint8_t* rgb8;        // image, written directly when spp == 1
+  double* sample_rgb;   // 3*n linear sample colours, reduced per pixel when spp > 1
+};
+
+// Device-side counters of one render (reset before each launch).
+struct DevControl {
+  unsigned long long next_ray;   // work queue head
+  unsigned long long attempts;   // step() calls, all rays
+  unsigned long long accepted;
+  unsigned long long class_count[5];
+  unsigned long long budget_used;
+  unsigned int abort;            // set once the attempt budget is spent
+  unsigned int pad;
+};
+
+}  // namespace gg

@@ -1,0 +1,277 @@
+"""Host mirror of gargantua's ``raytracer::curved`` render API over the C ABI.
+
+``render`` and ``render_with_disk`` keep the reference signatures
+(crates/raytracer/src/curved/renderer.rs:82-101) and return the image as a
+``uint8`` array of shape (height, width, 3), the ``RgbImage`` layout.  They
+run the CUDA library; there is no CPU path.
+
+Extensions beyond the reference (all opt-in through ``RenderOptions`` or
+``Scene``): a thin equatorial disk, a seeded checkerboard sky, seeded
+jittered samples, a configurable step budget and integrator, the mixed
+FP32/FP64 precision form, and per-sample outcome arrays.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+from typing import Optional, Union
+
+import numpy as np
+
+from . import abi
+from .gr_core import Kerr, RK45Integrator, Schwarzschild, renderer_integrator
+
+Metric = Union[Schwarzschild, Kerr]
+
+
+@dataclass
+class Camera:
+    """Pinhole camera (crates/raytracer/src/curved/camera.rs:9-15)."""
+
+    position: tuple = (0.0, 30.0, math.pi / 2.0, 0.0)
+    look_at: tuple = (-1.0, 0.0, 0.0)
+    up: tuple = (0.0, 0.0, 1.0)
+    fov_y_radians: float = math.radians(60.0)
+    aspect: float = 1.0
+
+    @classmethod
+    def inclined(cls, r: float, inclination: float, fov_y_radians: float,
+                 aspect: float) -> "Camera":
+        """Camera at (0, r, inclination, 0) looking at the hole with +z up."""
+        c = abi.gg_camera_t()
+        abi.check(abi.load().gg_camera_inclined(C.byref(c), r, inclination, fov_y_radians,
+                                                aspect), "gg_camera_inclined")
+        return cls(tuple(c.position), tuple(c.look_at), tuple(c.up), c.fov_y_radians, c.aspect)
+
+    def to_c(self) -> abi.gg_camera_t:
+        c = abi.gg_camera_t()
+        c.position[:] = [float(x) for x in self.position]
+        c.look_at[:] = [float(x) for x in self.look_at]
+        c.up[:] = [float(x) for x in self.up]
+        c.fov_y_radians = float(self.fov_y_radians)
+        c.aspect = float(self.aspect)
+        return c
+
+
+@dataclass
+class AccretionDisk:
+    """Volumetric Gaussian disk (crates/raytracer/src/curved/disk.rs:8-31)."""
+
+    r_inner: float = 6.0
+    r_outer: float = 20.0
+    scale_height: float = 1.0
+    density_0: float = 1.0
+    temperature_0: float = 1.0
+
+    def to_c(self) -> abi.gg_disk_t:
+        d = abi.gg_disk_t()
+        d.kind = abi.GG_DISK_VOLUMETRIC
+        d.r_inner, d.r_outer = self.r_inner, self.r_outer
+        d.scale_height, d.density_0 = self.scale_height, self.density_0
+        d.temperature_0 = self.temperature_0
+        return d
+
+
+@dataclass
+class ThinDisk:
+    """Thin equatorial disk: a ray ends at its first theta = pi/2 crossing with
+    r in [r_inner, r_outer]; observed intensity g^4 (r_inner / r)^q and colour
+    temperature g (r_inner / r)^(3/4), g the redshift of renderer's
+    ``redshift_factor`` (tracer.rs:158-183)."""
+
+    r_inner: float = 6.0
+    r_outer: float = 20.0
+    emissivity_index: float = 3.0
+
+    def to_c(self) -> abi.gg_disk_t:
+        d = abi.gg_disk_t()
+        d.kind = abi.GG_DISK_THIN
+        d.r_inner, d.r_outer = self.r_inner, self.r_outer
+        d.emissivity_index = self.emissivity_index
+        d.temperature_0 = 1.0
+        return d
+
+
+@dataclass
+class ProceduralSky:
+    """The reference's hashed starfield (crates/raytracer/src/curved/sky.rs:19-41)."""
+
+
+@dataclass
+class CheckerSky:
+    """Seeded checkerboard over the escape point's (theta, phi)."""
+
+    rows: int = 18
+    cols: int = 36
+    seed: int = 0
+
+
+@dataclass
+class RenderOptions:
+    """``RenderOptions`` (renderer.rs:17-26) plus the extensions listed above."""
+
+    samples_per_axis: int = 1
+    show_progress: bool = False
+    sky: Union[ProceduralSky, CheckerSky, None] = None
+    jitter_spp: int = 0
+    seed: int = 0
+    max_steps: int = 5000
+    integrator: Optional[RK45Integrator] = None
+    precision: int = abi.GG_PREC_FP64
+    attempt_budget: int = 0
+
+    def to_c(self) -> abi.gg_render_opts_t:
+        o = abi.gg_render_opts_t()
+        o.samples_per_axis = max(1, int(self.samples_per_axis))
+        o.jitter_spp = int(self.jitter_spp)
+        o.seed = int(self.seed) & (2**64 - 1)
+        sky = self.sky or ProceduralSky()
+        if isinstance(sky, CheckerSky):
+            o.sky, o.sky_rows, o.sky_cols = abi.GG_SKY_CHECKER, sky.rows, sky.cols
+            o.sky_seed = int(sky.seed) & (2**64 - 1)
+        else:
+            o.sky, o.sky_rows, o.sky_cols, o.sky_seed = abi.GG_SKY_PROCEDURAL, 18, 36, 0
+        o.attempt_budget = int(self.attempt_budget)
+        return o
+
+
+@dataclass
+class Scene:
+    """Everything one render call needs, as the C ABI takes it."""
+
+    metric: Metric
+    camera: Camera
+    width: int
+    height: int
+    disk: Union[AccretionDisk, ThinDisk, None] = None
+    options: RenderOptions = field(default_factory=RenderOptions)
+
+    @property
+    def spp(self) -> int:
+        o = self.options
+        return o.jitter_spp if o.jitter_spp > 0 else max(1, o.samples_per_axis) ** 2
+
+    @property
+    def n_samples(self) -> int:
+        return self.width * self.height * self.spp
+
+    def integrator_c(self) -> abi.gg_integrator_t:
+        integ = self.options.integrator or renderer_integrator()
+        return integ.to_c(self.options.max_steps, self.options.precision)
+
+    def c_structs(self):
+        return (self.metric.to_c(), self.camera.to_c(),
+                self.disk.to_c() if self.disk is not None else None, self.integrator_c(),
+                self.options.to_c())
+
+    def c_args(self):
+        m, c, d, i, o = self.c_structs()
+        self._keep = (m, c, d, i, o)
+        return (C.byref(m), C.byref(c), C.byref(d) if d is not None else None, C.byref(i),
+                C.byref(o), C.c_uint32(self.width), C.c_uint32(self.height))
+
+
+class RayOutputs:
+    """Host arrays of per-sample outcomes (``gg_ray_out_t``)."""
+
+    def __init__(self, n: int):
+        self.n = n
+        self.cls = np.full(n, -1, np.int32)
+        self.x = np.zeros((4, n), np.float64)
+        self.v = np.zeros((4, n), np.float64)
+        self.lam = np.zeros(n, np.float64)
+        self.attempts = np.zeros(n, np.uint32)
+        self.accepted = np.zeros(n, np.uint32)
+        self.intensity = np.zeros(n, np.float64)
+        self.color_temp = np.zeros(n, np.float64)
+        self.rgb = np.zeros((n, 3), np.float64)
+        self.cross = np.zeros((8, n), np.float64)
+
+    def struct(self) -> abi.gg_ray_out_t:
+        def p(a, t):
+            return a.ctypes.data_as(C.POINTER(t))
+        return abi.gg_ray_out_t(p(self.cls, C.c_int32), p(self.x, C.c_double),
+                                p(self.v, C.c_double), p(self.lam, C.c_double),
+                                p(self.attempts, C.c_uint32), p(self.accepted, C.c_uint32),
+                                p(self.intensity, C.c_double), p(self.color_temp, C.c_double),
+                                p(self.rgb, C.c_double), p(self.cross, C.c_double))
+
+
+class Renderer:
+    """One library context (one CUDA stream) on one device."""
+
+    def __init__(self, device: int = 0):
+        self._lib = abi.load()
+        h = C.c_void_p()
+        abi.check(self._lib.gg_create(C.byref(h), int(device)), "gg_create")
+        self._h = h
+
+    def close(self) -> None:
+        if self._h:
+            self._lib.gg_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    @property
+    def stream(self) -> int:
+        return self._lib.gg_stream(self._h) or 0
+
+    def render(self, scene: Scene, rays: bool = False):
+        """Synchronous render into host memory: (image, RayOutputs or None)."""
+        img = np.zeros((scene.height, scene.width, 3), np.uint8)
+        out = RayOutputs(scene.n_samples) if rays else None
+        st = self._lib.gg_render(self._h, *scene.c_args(), img.ctypes.data_as(C.c_void_p),
+                                 C.byref(out.struct()) if out else None)
+        abi.check(st, "gg_render")
+        return img, out
+
+    def render_device(self, scene: Scene, rgb_dev: int, rays_dev: abi.gg_ray_out_t | None = None,
+                      stream: int | None = None) -> None:
+        """Enqueue a render writing device pointers (no synchronisation)."""
+        st = self._lib.gg_render_device(self._h, *scene.c_args(), C.c_void_p(rgb_dev),
+                                        C.byref(rays_dev) if rays_dev is not None else None,
+                                        C.c_void_p(stream) if stream else None)
+        abi.check(st, "gg_render_device")
+
+    def stats(self) -> abi.gg_stats_t:
+        s = abi.gg_stats_t()
+        abi.check(self._lib.gg_last_stats(self._h, C.byref(s)), "gg_last_stats")
+        return s
+
+
+_DEFAULT: Optional[Renderer] = None
+
+
+def _renderer() -> Renderer:
+    global _DEFAULT
+    if _DEFAULT is None:
+        _DEFAULT = Renderer(0)
+    return _DEFAULT
+
+
+def render(metric: Metric, camera: Camera, width: int, height: int,
+           opts: Optional[RenderOptions] = None) -> np.ndarray:
+    """``render`` (renderer.rs:82-90): sky / horizon only."""
+    scene = Scene(metric, camera, width, height, None, opts or RenderOptions())
+    return _renderer().render(scene)[0]
+
+
+def render_with_disk(metric: Metric, camera: Camera, disk: Union[AccretionDisk, ThinDisk],
+                     width: int, height: int, opts: Optional[RenderOptions] = None) -> np.ndarray:
+    """``render_with_disk`` (renderer.rs:92-101)."""
+    scene = Scene(metric, camera, width, height, disk, opts or RenderOptions())
+    return _renderer().render(scene)[0]
+
+
+__all__ = ["Camera", "AccretionDisk", "ThinDisk", "ProceduralSky", "CheckerSky",
+           "RenderOptions", "Scene", "RayOutputs", "Renderer", "render", "render_with_disk"]

@@ -1,0 +1,218 @@
+/*
+ * gargantua_gpu.h -- C ABI of the B200 (sm_100a) general-relativistic ray path.
+ *
+ * The library renders images of a Schwarzschild or Kerr black hole by
+ * integrating one null geodesic per image sample on the GPU with the
+ * gargantua RK45 (Dormand-Prince) stepper, ends each ray at the horizon, the
+ * accretion disk or the escape sphere, and shades it.  Every entry point is
+ * plain C: POD structs, raw pointers and sizes, an int status.  No call
+ * aborts, panics or traps; failures come back as a negative status.
+ *
+ * Reference interface each group replaces (paths are inside gargantua):
+ *   gg_metric_*        gr-core  Metric impls   crates/gr-core/src/schwarzschild.rs:12-23,
+ *                                              crates/gr-core/src/kerr.rs:24-34
+ *   gg_integrator_*    gr-core  RK45Integrator crates/gr-core/src/geodesic.rs:155-181
+ *                      plus the renderer's overrides
+ *                                              crates/raytracer/src/curved/renderer.rs:264-265
+ *   gg_camera_t        raytracer::curved::Camera crates/raytracer/src/curved/camera.rs:9-15
+ *   gg_disk_t          raytracer::curved::AccretionDisk crates/raytracer/src/curved/disk.rs:8-31
+ *   gg_render          raytracer::curved::render / render_with_disk
+ *                                              crates/raytracer/src/curved/renderer.rs:82-101
+ *   gg_ray_out_t       raytracer::curved::RayOutcome crates/raytracer/src/curved/outcome.rs:4-22
+ *                      plus the final GeodesicState crates/gr-core/src/geodesic.rs:13-30
+ *
+ * Threading: one gg_ctx per host thread.  A context owns one CUDA stream and
+ * the device scratch it grows on demand; calls on one context are serialised.
+ */
+#ifndef GARGANTUA_GPU_H
+#define GARGANTUA_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define GG_API __attribute__((visibility("default")))
+#else
+#define GG_API
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define GG_OK 0
+#define GG_ERR_INVALID_ARG (-1) /* a parameter fails validation            */
+#define GG_ERR_CUDA (-2)        /* a CUDA runtime call failed              */
+#define GG_ERR_OOM (-3)         /* device allocation failed                */
+#define GG_ERR_BUDGET (-4)      /* the attempt budget ran out mid-render   */
+#define GG_ERR_UNSUPPORTED (-5) /* combination not implemented             */
+#define GG_ERR_NO_DEVICE (-6)   /* no CUDA device / not an sm_100 device   */
+
+/* ---- metric (gr-core Metric implementations) --------------------------- */
+#define GG_METRIC_SCHWARZSCHILD 0
+#define GG_METRIC_KERR 1
+
+typedef struct gg_metric_t {
+  int32_t kind;  /* GG_METRIC_* */
+  int32_t reserved;
+  double mass;   /* M > 0 */
+  double spin;   /* Kerr a, clamped to |a| <= 0.9999 M by gg_metric_kerr */
+} gg_metric_t;
+
+/* ---- camera (raytracer::curved::Camera) -------------------------------- */
+typedef struct gg_camera_t {
+  double position[4]; /* (t, r, theta, phi) in the metric's chart          */
+  double look_at[3];  /* local Cartesian frame, projected on r,theta,phi    */
+  double up[3];
+  double fov_y_radians;
+  double aspect;      /* width / height of the image plane                  */
+} gg_camera_t;
+
+/* ---- accretion disk ---------------------------------------------------- */
+#define GG_DISK_NONE 0       /* render(): trace_ray                            */
+#define GG_DISK_VOLUMETRIC 1 /* render_with_disk(): Gaussian volumetric disk   */
+#define GG_DISK_THIN 2       /* thin equatorial disk, emissivity (r_in/r)^q    */
+
+typedef struct gg_disk_t {
+  int32_t kind; /* GG_DISK_* */
+  int32_t reserved;
+  double r_inner;
+  double r_outer;
+  double scale_height;     /* volumetric: Gaussian H                        */
+  double density_0;        /* volumetric: rho_0                             */
+  double temperature_0;    /* volumetric: reported colour temperature       */
+  double emissivity_index; /* thin: q in I_emit = (r_inner / r)^q           */
+} gg_disk_t;
+
+/* ---- integrator (gr-core RK45Integrator + renderer loop bound) ---------- */
+#define GG_PREC_FP64 0  /* plain FP64, the drop-in                           */
+#define GG_PREC_MIXED 1 /* FP32 stages + compensated state, FP64 controller  */
+
+typedef struct gg_integrator_t {
+  double initial_step;
+  double min_step;
+  double max_step;
+  double tolerance;      /* absolute velocity-error tolerance (rtol == 0)    */
+  double max_radius;     /* escape radius                                    */
+  double horizon_buffer; /* Horizon when r < r_h + horizon_buffer            */
+  double rtol;           /* > 0: scaled error norm, atol + rtol*max(|v|,|v'|) */
+  double atol;
+  uint32_t max_steps;    /* step() calls per ray before MaxSteps             */
+  int32_t precision;     /* GG_PREC_*                                        */
+} gg_integrator_t;
+
+/* ---- render options (raytracer::curved::RenderOptions) ----------------- */
+#define GG_SKY_PROCEDURAL 0 /* hashed starfield over a blue gradient          */
+#define GG_SKY_CHECKER 1    /* seeded checkerboard over (theta, phi) cells     */
+
+typedef struct gg_render_opts_t {
+  uint32_t samples_per_axis; /* stratified supersampling, spa*spa per pixel */
+  uint32_t jitter_spp;       /* 0: stratified; n>0: n seeded uniform offsets */
+  uint64_t seed;             /* jitter seed                                 */
+  int32_t sky;               /* GG_SKY_*                                    */
+  uint32_t sky_rows;         /* checkerboard cells in theta (18)            */
+  uint32_t sky_cols;         /* checkerboard cells in phi (36)              */
+  uint32_t reserved;
+  uint64_t sky_seed;
+  uint64_t attempt_budget;   /* 0: unlimited; else GG_ERR_BUDGET past it    */
+} gg_render_opts_t;
+
+/* ---- per-sample outcome (RayOutcome + final GeodesicState) ------------- */
+#define GG_CLASS_HORIZON 0
+#define GG_CLASS_ESCAPED 1
+#define GG_CLASS_DISK 2
+#define GG_CLASS_MAXSTEPS 3
+#define GG_CLASS_BUDGET 4 /* not traced: the attempt budget ran out         */
+
+/* Every pointer is optional (NULL: not written).  Arrays have one entry per
+ * sample, ordered sample-major inside a pixel and pixels row-major:
+ * index = (py * width + px) * spp + s, with spp = spa*spa (s = sy*spa + sx)
+ * or jitter_spp.  x and v are component-major: x[c * n + i]. */
+typedef struct gg_ray_out_t {
+  int32_t* cls;        /* GG_CLASS_*                                      */
+  double* x;           /* 4*n final position (t, r, theta, phi)           */
+  double* v;           /* 4*n final velocity (dt, dr, dtheta, dphi)/dlam  */
+  double* lambda;      /* n affine parameter                              */
+  uint32_t* attempts;  /* n step() calls                                  */
+  uint32_t* accepted;  /* n accepted steps                                */
+  double* intensity;   /* n disk intensity (0 if none)                    */
+  double* color_temp;  /* n disk colour temperature (0 if none)           */
+  double* rgb;         /* 3*n linear colour of the sample, interleaved    */
+  double* cross;       /* 8*n state (x, v) where the ray met the escape
+                        * sphere r = max_radius or the thin disk plane,
+                        * interpolated on the last accepted step; NaN for
+                        * rays that ended elsewhere; component-major       */
+} gg_ray_out_t;
+
+/* ---- statistics of the last render on a context ------------------------ */
+typedef struct gg_stats_t {
+  uint64_t rays;
+  uint64_t attempts;
+  uint64_t accepted;
+  uint64_t class_count[5];
+  double kernel_ms; /* device time of the trace launch                      */
+} gg_stats_t;
+
+typedef struct gg_ctx gg_ctx;
+
+/* ---- library ----------------------------------------------------------- */
+GG_API const char* gg_version(void);
+GG_API const char* gg_strerror(int status);
+/* sizeof of a public struct by name ("gg_metric_t", ...), -1 if unknown */
+GG_API int gg_struct_size(const char* name);
+
+/* ---- parameter constructors (host only, no device work) ---------------- */
+/* Schwarzschild::new(mass) (schwarzschild.rs:13-18) */
+GG_API int gg_metric_schwarzschild(gg_metric_t* out, double mass);
+/* Kerr::new(mass, spin) (kerr.rs:29-34): mass <= 0 is GG_ERR_INVALID_ARG
+ * where the reference asserts; spin is clamped to +-0.9999 mass. */
+GG_API int gg_metric_kerr(gg_metric_t* out, double mass, double spin);
+/* RK45Integrator::default() (geodesic.rs:170-181) with the renderer's
+ * max_radius = 200 and max_steps = 5000 (renderer.rs:264-265). */
+GG_API void gg_integrator_default(gg_integrator_t* out);
+/* AccretionDisk::default() (disk.rs:21-31) as a volumetric disk. */
+GG_API void gg_disk_default(gg_disk_t* out);
+/* RenderOptions::default() with samples_per_axis = 1 (renderer.rs:267). */
+GG_API void gg_render_opts_default(gg_render_opts_t* out);
+/* Pinhole camera at (0, r, incl, 0) looking at the hole, up = +z. */
+GG_API int gg_camera_inclined(gg_camera_t* out, double r, double inclination_rad,
+                              double fov_y_radians, double aspect);
+/* Prograde ISCO (Bardeen-Press-Teukolsky) and prograde circular photon
+ * orbit radii of a Kerr hole; a = 0 gives 6M and 3M. */
+GG_API double gg_kerr_isco(double mass, double spin);
+GG_API double gg_kerr_photon_orbit(double mass, double spin);
+/* Checks every field a render would use; GG_OK or GG_ERR_INVALID_ARG. */
+GG_API int gg_validate(const gg_metric_t* metric, const gg_camera_t* camera,
+                       const gg_disk_t* disk, const gg_integrator_t* integ,
+                       const gg_render_opts_t* opts, uint32_t width, uint32_t height);
+
+/* ---- context ----------------------------------------------------------- */
+GG_API int gg_create(gg_ctx** out, int device);
+GG_API int gg_destroy(gg_ctx* ctx);
+/* The context's CUDA stream (a cudaStream_t). */
+GG_API void* gg_stream(gg_ctx* ctx);
+GG_API int gg_last_stats(gg_ctx* ctx, gg_stats_t* out);
+
+/* ---- rendering --------------------------------------------------------- */
+/* Drop-in for render / render_with_disk (renderer.rs:82-101).  Synchronous.
+ * rgb_out: host, width*height*3 bytes row-major (RgbImage layout), may be
+ * NULL.  rays_out: host arrays, may be NULL.  disk may be NULL (no disk). */
+GG_API int gg_render(gg_ctx* ctx, const gg_metric_t* metric, const gg_camera_t* camera,
+                     const gg_disk_t* disk, const gg_integrator_t* integ,
+                     const gg_render_opts_t* opts, uint32_t width, uint32_t height,
+                     uint8_t* rgb_out, const gg_ray_out_t* rays_out);
+
+/* Same render with DEVICE output pointers, enqueued on `stream` (a
+ * cudaStream_t; NULL = the context's stream) without synchronising.
+ * Scratch comes from the context. */
+GG_API int gg_render_device(gg_ctx* ctx, const gg_metric_t* metric, const gg_camera_t* camera,
+                            const gg_disk_t* disk, const gg_integrator_t* integ,
+                            const gg_render_opts_t* opts, uint32_t width, uint32_t height,
+                            uint8_t* rgb_dev, const gg_ray_out_t* rays_dev, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GARGANTUA_GPU_H */

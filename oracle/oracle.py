@@ -1,0 +1,160 @@
+"""Python loader of the CPU oracle (``oracle/_build/liboracle_gg.so``).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, ``__graft_entry__.smoke`` and the
+CPU-baseline leg of ``bench.py`` as the checker; the product never imports it.
+The parameter structs are the product ABI's POD structs so both sides trace
+identical inputs.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+from gargantua_b200 import abi
+
+ORACLE_DIR = Path(__file__).resolve().parent
+LIB_PATH = ORACLE_DIR / "_build" / "liboracle_gg.so"
+
+P = C.POINTER
+D4 = C.c_double * 4
+
+
+def build() -> Path:
+    subprocess.run(["make", "-s", "-C", str(ORACLE_DIR)], check=True)
+    return LIB_PATH
+
+
+_LIB = None
+
+
+def lib() -> C.CDLL:
+    global _LIB
+    if _LIB is None:
+        if not LIB_PATH.exists():
+            build()
+        L = C.CDLL(str(LIB_PATH))
+        common = [P(abi.gg_metric_t), P(abi.gg_camera_t), P(abi.gg_disk_t),
+                  P(abi.gg_integrator_t), P(abi.gg_render_opts_t), C.c_uint32, C.c_uint32]
+        sig = {
+            "ggo_render": (C.c_int, common + [C.c_void_p, P(abi.gg_ray_out_t), C.c_int]),
+            "ggo_trace_samples": (C.c_int, common + [C.c_void_p, C.c_uint64,
+                                                     P(abi.gg_ray_out_t), C.c_int]),
+            "ggo_trace_cross": (C.c_int, common + [C.c_void_p, C.c_uint64, C.c_void_p,
+                                                   C.c_int]),
+            "ggo_trace_state": (C.c_int, common[:5] + [C.c_void_p, P(abi.gg_ray_out_t)]),
+            "ggo_trace_uv": (C.c_int, common[:5] + [C.c_double, C.c_double,
+                                                    P(abi.gg_ray_out_t)]),
+            "ggo_metric_tensor": (C.c_int, [P(abi.gg_metric_t), C.c_void_p, C.c_void_p]),
+            "ggo_christoffel": (C.c_int, [P(abi.gg_metric_t), C.c_void_p, C.c_void_p]),
+            "ggo_numerical_christoffel": (C.c_int, [P(abi.gg_metric_t), C.c_void_p,
+                                                    C.c_double, C.c_void_p]),
+            "ggo_geodesic_acceleration": (C.c_int, [P(abi.gg_metric_t), C.c_void_p,
+                                                    C.c_void_p, C.c_void_p]),
+            "ggo_event_horizon": (C.c_int, [P(abi.gg_metric_t), P(C.c_double)]),
+            "ggo_orbital_four_velocity": (C.c_int, [P(abi.gg_metric_t), C.c_void_p,
+                                                    C.c_void_p]),
+            "ggo_rk4_run": (C.c_int, [P(abi.gg_metric_t), C.c_void_p, C.c_double,
+                                      C.c_uint64]),
+            "ggo_rk45_step": (C.c_int, [P(abi.gg_metric_t), P(abi.gg_integrator_t),
+                                        C.c_void_p, P(C.c_double), P(C.c_int)]),
+            "ggo_count_attempt_ops": (C.c_int, [P(abi.gg_metric_t), P(abi.gg_integrator_t),
+                                                C.c_void_p, C.c_double, C.c_void_p]),
+            "ggo_pixel_direction": (None, [P(abi.gg_camera_t), C.c_double, C.c_double,
+                                           C.c_void_p]),
+            "ggo_from_camera": (C.c_int, [P(abi.gg_metric_t), P(abi.gg_camera_t), C.c_uint32,
+                                          C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p]),
+            "ggo_redshift_factor": (C.c_double, [P(abi.gg_metric_t), C.c_void_p, C.c_void_p,
+                                                 C.c_double]),
+            "ggo_procedural_sky": (None, [C.c_void_p, C.c_void_p]),
+            "ggo_checker_sky": (None, [C.c_double, C.c_double, C.c_uint32, C.c_uint32,
+                                       C.c_uint64, C.c_void_p]),
+            "ggo_disk_color": (None, [C.c_double, C.c_void_p]),
+            "ggo_encode_srgb": (None, [C.c_void_p, C.c_void_p]),
+            "ggo_splitmix64": (C.c_uint64, [C.c_uint64]),
+            "ggo_sample_uv": (None, [P(abi.gg_render_opts_t), C.c_uint32, C.c_uint32,
+                                     C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p]),
+            "ggo_kerr_isco": (C.c_double, [C.c_double, C.c_double]),
+            "ggo_kerr_photon_orbit": (C.c_double, [C.c_double, C.c_double]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _LIB = L
+    return _LIB
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+from gargantua_b200.curved import RayOutputs as RayArrays  # noqa: E402
+
+
+def render(scene, threads: int = 0, rays: bool = True):
+    """Render ``scene`` (a ``gargantua_b200.curved.Scene``) on the CPU oracle.
+
+    Returns (rgb uint8 [H, W, 3], RayArrays or None)."""
+    w, h = scene.width, scene.height
+    n = w * h * scene.spp
+    img = np.zeros((h, w, 3), np.uint8)
+    ra = RayArrays(n) if rays else None
+    st = lib().ggo_render(*scene.c_args(), _ptr(img), C.byref(ra.struct()) if ra else None,
+                          threads)
+    abi.check(st, "ggo_render")
+    return img, ra
+
+
+def trace_samples(scene, index: np.ndarray, threads: int = 0) -> RayArrays:
+    index = np.ascontiguousarray(index, np.uint64)
+    ra = RayArrays(len(index))
+    st = lib().ggo_trace_samples(*scene.c_args(), _ptr(index), len(index),
+                                 C.byref(ra.struct()), threads)
+    abi.check(st, "ggo_trace_samples")
+    return ra
+
+
+def trace_uv(scene, u: float, v: float) -> RayArrays:
+    ra = RayArrays(1)
+    st = lib().ggo_trace_uv(*scene.c_args()[:5], u, v, C.byref(ra.struct()))
+    abi.check(st, "ggo_trace_uv")
+    return ra
+
+
+def sample_uv(scene, index: int) -> tuple[float, float]:
+    spp = scene.spp
+    pix, s = divmod(int(index), spp)
+    py, px = divmod(pix, scene.width)
+    uv = np.zeros(2)
+    o = scene.options.to_c()
+    lib().ggo_sample_uv(C.byref(o), scene.width, scene.height, px, py, s, _ptr(uv))
+    return float(uv[0]), float(uv[1])
+
+
+def near_class_boundary(scene, index: int, margin_m: float = 1e-6) -> bool:
+    """True when re-shooting sample `index` with its image-plane point moved by
+    an impact-parameter offset of `margin_m` (in units of M) in +-u or +-v
+    changes its termination class: the sample lies on a class boundary."""
+    u, v = sample_uv(scene, index)
+    cam = scene.camera
+    half_h = np.tan(cam.fov_y_radians / 2.0)
+    half_w = half_h * cam.aspect
+    r_cam = cam.position[1]
+    du = margin_m / (r_cam * half_w)
+    dv = margin_m / (r_cam * half_h)
+    base = trace_uv(scene, u, v).cls[0]
+    for uu, vv in ((u + du, v), (u - du, v), (u, v + dv), (u, v - dv)):
+        if trace_uv(scene, uu, vv).cls[0] != base:
+            return True
+    return False
+
+
+def trace_cross(scene, index: np.ndarray, threads: int = 0) -> np.ndarray:
+    index = np.ascontiguousarray(index, np.uint64)
+    out = np.zeros((8, len(index)), np.float64)
+    st = lib().ggo_trace_cross(*scene.c_args(), _ptr(index), len(index), _ptr(out), threads)
+    abi.check(st, "ggo_trace_cross")
+    return out
