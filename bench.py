@@ -1,0 +1,354 @@
+#!/usr/bin/env python3
+"""Kerr 1080p geodesics/s on B200: plain FP64 and mixed FP32/FP64 forms.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: Kerr a = 0.9, 1920x1080, 1 sample per pixel, camera r = 50 M at 75
+deg inclination, 60 deg FOV, thin disk r_ISCO-30 M (q = 3), seeded 18x36
+checkerboard sky, RK45 with rtol 1e-8 / atol 1e-10, 10,000 step() calls per
+ray, escape at r = 200.  A step is one full render of that frame; the scene
+is procedural (nothing to load), so "inputs resident" means the parameter
+block only.  Between timed steps a 256 MiB buffer is written to flush L2.
+
+One JSON line on rank 0.  ``value`` is whole-job geodesics/s (rays traced to
+termination per second, summed over ranks; each rank renders its own frame:
+weak scaling, no collective on the data path).  ``e2e`` is the same metric
+through the public synchronous call ``gg_render`` into pinned host memory
+(parameters in, sRGB image out, copies inside the timed region).
+
+``--impl reference`` times the CPU restatement of the reference's renderer
+(the oracle; the Rust reference cannot be built here) on the host cores on
+a bounded seeded sample of the same frame.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Kerr 1080p geodesics/s, mixed-FP32 vs plain FP64 on B200 at stated endpoint error"
+UNIT = "geodesics/s"
+FLUSH_BYTES = 256 << 20
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def workload_config(scene, form: str) -> dict:
+    integ = scene.integrator_c()
+    return {"workload": "kerr_a0.9_1920x1080_thin_disk", "form": form,
+            "width": scene.width, "height": scene.height, "spp": scene.spp,
+            "spin": scene.metric.spin, "r_cam": scene.camera.position[1],
+            "inclination_deg": round(scene.camera.position[2] * 180.0 / 3.141592653589793, 6),
+            "disk": [scene.disk.r_inner, scene.disk.r_outer, scene.disk.emissivity_index],
+            "rtol": integ.rtol, "atol": integ.atol, "max_steps": integ.max_steps,
+            "max_radius": integ.max_radius, "sky": "checkerboard 18x36 seed 0",
+            "l2": "256 MiB write between timed steps"}
+
+
+# ---- clocks ------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        sel = []
+        try:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(device_index).uuid)
+            sel = ["-i", uuid if uuid.startswith("GPU-") else f"GPU-{uuid}"]
+        except Exception:
+            sel = []
+        self.p = None
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"] + sel,
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.p = None
+        time.sleep(0.3)
+
+    def stop(self) -> dict:
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.p.terminate()
+        try:
+            self.p.wait(5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.seek(0)
+        sm, smax, power, reasons = [], [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+                power.append(float(parts[3]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        os.unlink(self.f.name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax),
+                "power_w_max": max(power), "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# ---- our arm -------------------------------------------------------------------
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def time_form(r, scene, steps, warmup, world, flush, with_clocks, device_index):
+    """Device-timed renders of `scene` with device-resident outputs."""
+    import torch
+    out = torch.empty(scene.width * scene.height * 3, dtype=torch.uint8, device="cuda")
+    # everything (flush, events, renders) on the library context's own stream
+    stream = torch.cuda.ExternalStream(r.stream)
+    for _ in range(warmup):
+        r.render_device(scene, out.data_ptr(), None, r.stream)
+    stream.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(steps)]
+    barrier(world)
+    torch.cuda.synchronize()
+    clk = ClockSampler(device_index) if with_clocks else None
+    with torch.cuda.stream(stream):
+        for i in range(steps):
+            flush.zero_()
+            ev[i][0].record(stream)
+            r.render_device(scene, out.data_ptr(), None, r.stream)
+            ev[i][1].record(stream)
+    stream.synchronize()
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = clk.stop() if clk else None
+    ms = [a.elapsed_time(b) for a, b in ev]
+    st = r.stats()
+    total_ms = max_over_ranks(sum(ms), world)
+    return {"ms": ms, "total_ms": total_ms, "stats": st, "clocks": clocks}
+
+
+def time_e2e(r, scene, steps, warmup, world):
+    import numpy as np
+    import torch
+    host = torch.empty(scene.width * scene.height * 3, dtype=torch.uint8,
+                       pin_memory=True).numpy()
+    for _ in range(warmup):
+        r.render_into(scene, host)
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        r.render_into(scene, host)
+    t1 = time.perf_counter()
+    barrier(world)
+    el = max_over_ranks(t1 - t0, world)
+    assert np.any(host)
+    return el
+
+
+def cpu_baseline(scene, target_s: float = 10.0) -> dict:
+    import numpy as np
+    from oracle import oracle
+    rng = np.random.default_rng(0)
+    threads = len(os.sched_getaffinity(0))
+    probe = np.sort(rng.choice(scene.n_samples, 2048, replace=False)).astype(np.uint64)
+    t0 = time.perf_counter()
+    oracle.trace_samples(scene, probe, threads=threads)
+    rate = 2048 / (time.perf_counter() - t0)
+    n = int(min(scene.n_samples, max(4096, rate * target_s)))
+    idx = np.sort(rng.choice(scene.n_samples, n, replace=False)).astype(np.uint64)
+    t0 = time.perf_counter()
+    oracle.trace_samples(scene, idx, threads=threads)
+    el = time.perf_counter() - t0
+    return {"value": n / el, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{n} seeded rays of the 1920x1080 frame (rng seed 0), "
+                      f"{el:.1f} s on {threads} host threads"}
+
+
+def run_ours(args) -> None:
+    import numpy as np
+    import torch
+
+    from gargantua_b200 import abi, flops, workloads
+    from gargantua_b200.curved import Renderer
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device(f"cuda:{local}"))
+    steps, warmup = args.steps, max(3, args.warmup)
+    r = Renderer(local)
+    flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    forms = {}
+    for form, prec in (("fp64", abi.GG_PREC_FP64), ("mixed", abi.GG_PREC_MIXED)):
+        scene = workloads.kerr_thin_1080p(precision=prec)
+        try:
+            res = time_form(r, scene, steps, warmup, world, flush, True, local)
+        except abi.GargantuaError as e:
+            if e.status == abi.GG_ERR_UNSUPPORTED:
+                continue
+            raise
+        st = res["stats"]
+        mean_ms = statistics.mean(res["ms"])
+        forms[form] = {
+            "geodesics_per_s": world * scene.n_samples * steps / (res["total_ms"] * 1e-3),
+            "ms_per_step": res["total_ms"] / steps,
+            "launch_ms_mean": mean_ms,
+            "attempts_per_frame": int(st.attempts),
+            "accepted_per_frame": int(st.accepted),
+            "attempts_per_s": world * st.attempts * steps / (res["total_ms"] * 1e-3),
+            "accepted_steps_per_s": world * st.accepted * steps / (res["total_ms"] * 1e-3),
+            "class_count": [int(x) for x in st.class_count],
+            "clocks": res["clocks"], "scene": scene,
+        }
+    head = "mixed" if "mixed" in forms else "fp64"
+    H = forms[head]
+    scene = H["scene"]
+
+    # roofline of the trace kernel: counted reference FLOPs per attempt x attempts
+    fpa = flops.attempt_flops("kerr", scene.integrator_c().rtol)
+    fp64_peak = r.fma_peak(fp64=True)
+    fp32_peak = r.fma_peak(fp64=False)
+    peak = fp64_peak if head == "fp64" else fp32_peak
+    achieved = H["attempts_per_frame"] * fpa / (H["launch_ms_mean"] * 1e-3)
+
+    # end to end through gg_render (host pinned output)
+    e2e_s = time_e2e(r, scene, steps, warmup, world)
+
+    # per-ray attempt distribution (one untimed render with per-ray outputs)
+    _, rays = r.render(scene, rays=True)
+    pct = np.percentile(rays.attempts, [50, 90, 99, 99.9, 100]).tolist()
+
+    line = {
+        "metric": METRIC, "value": H["geodesics_per_s"], "unit": UNIT, "n_gpus": world,
+        "steps": steps, "warmup": warmup, "ms_per_step": H["ms_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if head == "fp64" else "f32+f64",
+        "data": "synthetic: procedural Kerr scene, seeded checkerboard sky",
+        "config": workload_config(scene, head),
+        "clocks": H["clocks"],
+        "e2e": {"value": world * scene.n_samples * steps / e2e_s, "unit": UNIT,
+                "h2d_bytes_per_step": abi.load().gg_struct_size(b"launch_params"),
+                "d2h_bytes_per_step": scene.width * scene.height * 3},
+        "gpu_launches": steps,
+        "roofline": {"bound": "fp64" if head == "fp64" else "fp32", "achieved": achieved / 1e12,
+                     "peak": peak / 1e12, "unit": "TFLOP/s", "frac": achieved / peak,
+                     "traffic": None, "kernel": f"trace_{head}_kernel<Kerr, ThinDisk>",
+                     "flops_per_attempt": fpa,
+                     "peak_source": "measured in this run by gg_measure_fma_peak (FMA chains);"
+                                    " MEASURED_PEAKS.json has no FP64/FP32 ALU figure"},
+        "forms": {k: {kk: vv for kk, vv in v.items() if kk not in ("scene", "clocks")}
+                  for k, v in forms.items()},
+        "fma_peak_tflops": {"fp64": fp64_peak / 1e12, "fp32": fp32_peak / 1e12},
+        "attempts_per_ray_pct": {"p50": pct[0], "p90": pct[1], "p99": pct[2], "p99.9": pct[3],
+                                 "max": pct[4]},
+    }
+    if "mixed" in forms and "fp64" in forms:
+        line["mixed_over_fp64"] = forms["mixed"]["geodesics_per_s"] / forms["fp64"]["geodesics_per_s"]
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(scene)
+    r.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+# ---- reference arm ---------------------------------------------------------------
+def run_reference(args) -> None:
+    import numpy as np
+
+    from gargantua_b200 import workloads
+    from oracle import oracle
+
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    scene = workloads.kerr_thin_1080p()
+    threads = len(os.sched_getaffinity(0))
+    rng = np.random.default_rng(0)
+    probe = np.sort(rng.choice(scene.n_samples, 2048, replace=False)).astype(np.uint64)
+    t0 = time.perf_counter()
+    oracle.trace_samples(scene, probe, threads=threads)
+    rate = 2048 / (time.perf_counter() - t0)
+    steps, warmup = args.steps, max(3, args.warmup)
+    per_step_s = min(20.0, 150.0 / (steps + warmup))
+    n = int(min(scene.n_samples, max(2048, rate * per_step_s)))
+    idx = np.sort(rng.choice(scene.n_samples, n, replace=False)).astype(np.uint64)
+    for _ in range(warmup):
+        oracle.trace_samples(scene, idx[: max(256, n // 8)], threads=threads)
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        oracle.trace_samples(scene, idx, threads=threads)
+        times.append(time.perf_counter() - t0)
+    value = n * steps / sum(times)
+    sample = (f"{n} seeded rays of the 1920x1080 frame per step (rng seed 0) on "
+              f"{threads} host threads; C++ f64 restatement of the reference renderer "
+              "(the Rust reference cannot be built here)")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+            "n_gpus": world, "steps": steps, "warmup": warmup,
+            "ms_per_step": 1e3 * sum(times) / steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: procedural Kerr scene, seeded checkerboard sky",
+            "config": workload_config(scene, "reference f64 CPU"),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -19,7 +19,7 @@ from pathlib import Path
 PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 OUT = PKG / "libgargantua_gpu.so"
-SOURCES = ["gg_trace.cu", "gg_capi.cpp"]
+SOURCES = ["gg_trace.cu", "gg_peak.cu", "gg_capi.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -39,24 +39,30 @@ def flags(verbose: bool = False) -> list[str]:
     return f
 
 
-def build(verbose: bool = False, force: bool = False) -> Path:
+def build(verbose: bool = False, force: bool = False, out: Path | None = None,
+          defines: tuple[str, ...] = ()) -> Path:
+    """Compiles the library to `out` (default: the in-tree package copy);
+    `defines` are extra -D macros (tuning knobs such as GG_TRACE_MIN_BLOCKS)."""
+    out = Path(out) if out is not None else OUT
     srcs = [CSRC / s for s in SOURCES]
     deps = srcs + list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + \
         [PKG.parent / "include" / "gargantua_gpu.h"]
-    if not force and OUT.exists() and not verbose:
+    if not force and out.exists() and not verbose and not defines:
         newest = max(p.stat().st_mtime for p in deps)
-        if OUT.stat().st_mtime >= newest:
-            return OUT
+        if out.stat().st_mtime >= newest:
+            return out
     with tempfile.TemporaryDirectory() as tmp:
-        tmp_out = Path(tmp) / OUT.name
-        cmd = [nvcc()] + flags(verbose) + [str(s) for s in srcs] + ["-o", str(tmp_out)]
+        tmp_out = Path(tmp) / out.name
+        cmd = [nvcc()] + flags(verbose) + [f"-D{d}" for d in defines] + \
+            [str(s) for s in srcs] + ["-o", str(tmp_out)]
         res = subprocess.run(cmd, capture_output=True, text=True)
         if verbose or res.returncode != 0:
             sys.stderr.write(res.stdout + res.stderr)
         if res.returncode != 0:
             raise RuntimeError(f"nvcc failed ({res.returncode}): {' '.join(cmd)}")
-        shutil.move(str(tmp_out), OUT)
-    return OUT
+        out.parent.mkdir(parents=True, exist_ok=True)
+        shutil.move(str(tmp_out), out)
+    return out
 
 
 if __name__ == "__main__":

@@ -364,7 +364,9 @@ GG_API int gg_struct_size(const char* name) {
            {"gg_integrator_t", (int)sizeof(gg_integrator_t)},
            {"gg_render_opts_t", (int)sizeof(gg_render_opts_t)},
            {"gg_ray_out_t", (int)sizeof(gg_ray_out_t)},
-           {"gg_stats_t", (int)sizeof(gg_stats_t)}};
+           {"gg_stats_t", (int)sizeof(gg_stats_t)},
+           // bytes that reach the device per render as kernel parameters
+           {"launch_params", (int)(sizeof(DevParams) + sizeof(DevOutputs) + sizeof(void*))}};
   for (auto& e : t)
     if (std::strcmp(e.n, name) == 0) return e.s;
   return -1;
@@ -519,6 +521,13 @@ GG_API int gg_last_stats(gg_ctx* c, gg_stats_t* out) {
   return st == GG_ERR_BUDGET ? GG_OK : st;
 }
 
+GG_API int gg_measure_fma_peak(gg_ctx* c, int fp64, double* flops) {
+  if (!c || !flops) return GG_ERR_INVALID_ARG;
+  Lock lock(c);
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return GG_ERR_CUDA;
+  return gg::measure_fma_peak(fp64, c->sms, flops) == cudaSuccess ? GG_OK : GG_ERR_CUDA;
+}
+
 GG_API int gg_render_device(gg_ctx* c, const gg_metric_t* metric, const gg_camera_t* camera,
                             const gg_disk_t* disk, const gg_integrator_t* integ,
                             const gg_render_opts_t* opts, uint32_t width, uint32_t height,
@@ -545,8 +554,8 @@ GG_API int gg_render_device(gg_ctx* c, const gg_metric_t* metric, const gg_camer
     O.cross = rays_dev->cross;
   }
   O.rgb8 = rgb_dev;
-  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
-  return enqueue(c, P, O, rgb_dev != nullptr, s);
+  // NULL is CUDA's default stream, as for any CUDA API taking a stream
+  return enqueue(c, P, O, rgb_dev != nullptr, static_cast<cudaStream_t>(stream));
 }
 
 GG_API int gg_render(gg_ctx* c, const gg_metric_t* metric, const gg_camera_t* camera,

@@ -35,100 +35,136 @@ GG_DEV double add_rn(double a, double b) { return __dadd_rn(a, b); }
 GG_DEV double sub_rn(double a, double b) { return __dsub_rn(a, b); }
 
 // ---------------------------------------------------------------------------
-// Geodesic right-hand side a^mu = -Gamma^mu_ab v^a v^b.
+// Geodesic right-hand side a^mu = -Gamma^mu_ab v^a v^b, split in two: the
+// position-dependent coefficients of the quadratic form (sincos, one
+// reciprocal, the metric derivatives and inverse metric) and the cheap
+// contraction with a velocity.  RK45's last two stages (k6 at pos6 with the
+// stage velocity, k7 at pos6 with the new velocity, geodesic.rs:284-298) share
+// the first part.
 // ---------------------------------------------------------------------------
 
-// Schwarzschild (schwarzschild.rs:99-140), one reciprocal.
-GG_DEV void rhs_schwarzschild(const DevParams& P, double r_in, double th, const double v[4],
-                              double a[4]) {
-  const double r = fmax(r_in, 1e-10);
-  double s, c;
-  sincos(th, &s, &c);
-  const double rs = P.rs;
-  const double rmrs = r - rs;
-  const double R = 1.0 / (r * rmrs * s);  // 1 / (r (r - rs) sin)
-  const double ifd = s * R;                // 1 / (r (r - rs))
-  const double ir = rmrs * ifd;            // 1 / r
-  const double is = (r * rmrs) * R;        // 1 / sin
-  const double g_t_tr = 0.5 * rs * ifd;
-  const double g_r_tt = 0.5 * rs * rmrs * (ir * ir * ir);
-  const double g_r_thth = -rmrs;
-  const double g_r_phph = -rmrs * s * s;
-  const double g_th_phph = -s * c;
-  const double g_ph_thph = c * is;
-  const double vt = v[0], vr = v[1], vth = v[2], vph = v[3];
-  a[0] = -2.0 * g_t_tr * vt * vr;
-  a[1] = -g_r_tt * vt * vt + g_t_tr * vr * vr - g_r_thth * vth * vth - g_r_phph * vph * vph;
-  a[2] = -2.0 * ir * vr * vth - g_th_phph * vph * vph;
-  a[3] = -2.0 * ir * vr * vph - 2.0 * g_ph_thph * vth * vph;
-}
-
 // Kerr in Boyer-Lindquist coordinates.  Metric derivatives are the
-// reference's (kerr.rs:154-204) with shared factors pulled out; the
-// contraction groups the symbols by row as described at the top.
+// reference's (kerr.rs:154-204) with shared factors pulled out and all of
+// 1/Sigma, 1/Delta, 1/sin^2 taken from one reciprocal.
 template <class T>
-GG_DEV void rhs_kerr_t(T M, T a, T r_in, T s, T c, const T v[4], T acc[4]) {
-  const T r = r_in;
+struct KerrGeo {
+  T dtt_r, dtt_th, drr_r, drr_th, dthth_r, dthth_th, dphph_r, dphph_th, dtph_r, dtph_th;
+  T gtt, gtph, gphph;  // inverse metric, (t, phi) block
+  T hrr, hthth;        // -g^rr / 2, -g^thth / 2
+};
+
+template <class T>
+GG_DEV KerrGeo<T> kerr_geometry(T M, T a, T r, T s, T c) {
+  KerrGeo<T> G;
   const T r2 = r * r, a2 = a * a, s2 = s * s, c2 = c * c, sc = s * c;
   const T sig = r2 + a2 * c2;
   const T del = (r - T(2) * M) * r + a2;
   const T rho = r2 + a2;
   const T sd = sig * del;
   const T R = T(1) / (sd * s2);
-  const T iSD = s2 * R;        // 1 / (Sigma Delta)
-  const T iS = del * iSD;      // 1 / Sigma
-  const T iD = sig * iSD;      // 1 / Delta
-  const T is2 = sd * R;        // 1 / sin^2
+  const T iSD = s2 * R;  // 1 / (Sigma Delta)
+  const T iS = del * iSD;  // 1 / Sigma
+  const T iD = sig * iSD;  // 1 / Delta
+  const T is2 = sd * R;    // 1 / sin^2
   const T iS2 = iS * iS;
   const T Mr = M * r;
-  // d_r and d_theta of g_tt, g_rr, g_thth, g_phph, g_tphi
   const T sm2r = a2 * c2 - r2;  // Sigma - 2 r^2
-  const T dtt_r = T(2) * M * sm2r * iS2;
-  const T dtt_th = T(4) * Mr * a2 * sc * iS2;
-  const T drr_r = T(2) * (a2 * (r * s2 + M * c2) - M * r2) * (iD * iD);
-  const T drr_th = T(-2) * a2 * sc * iD;
-  const T dthth_r = T(2) * r;
-  const T dthth_th = T(-2) * a2 * sc;
-  const T dphph_r = T(2) * r * s2 + T(2) * M * a2 * (s2 * s2) * sm2r * iS2;
-  const T dphph_th = T(2) * rho * sc + T(2) * Mr * a2 * sc * s2 * (T(2) * (sig + rho)) * iS2;
-  const T dtph_r = T(-2) * M * a * s2 * sm2r * iS2;
-  const T dtph_th = T(-4) * Mr * a * sc * rho * iS2;
-  // inverse metric
+  G.dtt_r = T(2) * M * sm2r * iS2;
+  G.dtt_th = T(4) * Mr * a2 * sc * iS2;
+  G.drr_r = T(2) * (a2 * (r * s2 + M * c2) - M * r2) * (iD * iD);
+  G.drr_th = T(-2) * a2 * sc * iD;
+  G.dthth_r = T(2) * r;
+  G.dthth_th = T(-2) * a2 * sc;
+  G.dphph_r = T(2) * r * s2 + T(2) * M * a2 * (s2 * s2) * sm2r * iS2;
+  G.dphph_th = T(2) * rho * sc + T(4) * Mr * a2 * sc * s2 * (sig + rho) * iS2;
+  G.dtph_r = T(-2) * M * a * s2 * sm2r * iS2;
+  G.dtph_th = T(-4) * Mr * a * sc * rho * iS2;
   const T big_a = rho * rho - a2 * del * s2;
-  const T gtt = -big_a * iSD;
-  const T gtph = T(-2) * Mr * a * iSD;
-  const T grr = del * iS;
-  const T gthth = iS;
-  const T gphph = (del - a2 * s2) * iSD * is2;
-  const T vt = v[0], vr = v[1], vth = v[2], vph = v[3];
-  const T Et = vr * (dtt_r * vt + dtph_r * vph) + vth * (dtt_th * vt + dtph_th * vph);
-  const T Ep = vr * (dtph_r * vt + dphph_r * vph) + vth * (dtph_th * vt + dphph_th * vph);
-  acc[0] = -(gtt * Et + gtph * Ep);
-  acc[3] = -(gtph * Et + gphph * Ep);
-  const T vt2 = vt * vt, vr2 = vr * vr, vth2 = vth * vth, vph2 = vph * vph;
-  const T two_tp = T(2) * vt * vph, two_rt = T(2) * vr * vth;
-  acc[1] = T(-0.5) * grr *
-           (drr_r * vr2 - dtt_r * vt2 - dthth_r * vth2 - dphph_r * vph2 + drr_th * two_rt -
-            dtph_r * two_tp);
-  acc[2] = T(-0.5) * gthth *
-           (dthth_th * vth2 - dtt_th * vt2 - drr_th * vr2 - dphph_th * vph2 +
-            dthth_r * two_rt - dtph_th * two_tp);
+  G.gtt = -big_a * iSD;
+  G.gtph = T(-2) * Mr * a * iSD;
+  G.gphph = (del - a2 * s2) * iSD * is2;
+  G.hrr = T(-0.5) * del * iS;
+  G.hthth = T(-0.5) * iS;
+  return G;
 }
 
-GG_DEV void rhs_kerr(const DevParams& P, double r_in, double th, const double v[4],
-                     double a[4]) {
-  double s, c;
-  sincos(th, &s, &c);
-  rhs_kerr_t<double>(P.mass, P.spin, fmax(r_in, 1e-10), s, c, v, a);
+// t and phi rows share the "energy" sums E_t, E_phi; the r and theta rows
+// their -g^ii / 2 factor.
+template <class T>
+GG_DEV void kerr_contract(const KerrGeo<T>& G, const T v[4], T acc[4]) {
+  const T vt = v[0], vr = v[1], vth = v[2], vph = v[3];
+  const T Et = vr * (G.dtt_r * vt + G.dtph_r * vph) + vth * (G.dtt_th * vt + G.dtph_th * vph);
+  const T Ep = vr * (G.dtph_r * vt + G.dphph_r * vph) + vth * (G.dtph_th * vt + G.dphph_th * vph);
+  acc[0] = -(G.gtt * Et + G.gtph * Ep);
+  acc[3] = -(G.gtph * Et + G.gphph * Ep);
+  const T vt2 = vt * vt, vr2 = vr * vr, vth2 = vth * vth, vph2 = vph * vph;
+  const T two_tp = T(2) * vt * vph, two_rt = T(2) * vr * vth;
+  acc[1] = G.hrr * (G.drr_r * vr2 - G.dtt_r * vt2 - G.dthth_r * vth2 - G.dphph_r * vph2 +
+                    G.drr_th * two_rt - G.dtph_r * two_tp);
+  acc[2] = G.hthth * (G.dthth_th * vth2 - G.dtt_th * vt2 - G.drr_th * vr2 - G.dphph_th * vph2 +
+                      G.dthth_r * two_rt - G.dtph_th * two_tp);
+}
+
+// Schwarzschild (schwarzschild.rs:99-140): 9 non-zero symbols, one reciprocal.
+struct SchwGeo {
+  double g_t_tr, g_r_tt, g_r_thth, g_r_phph, ir, g_th_phph, g_ph_thph;
+};
+
+GG_DEV SchwGeo schw_geometry(double rs, double r, double s, double c) {
+  SchwGeo G;
+  const double rmrs = r - rs;
+  const double R = 1.0 / (r * rmrs * s);  // 1 / (r (r - rs) sin)
+  const double ifd = s * R;                // 1 / (r (r - rs))
+  G.ir = rmrs * ifd;                       // 1 / r
+  const double is = (r * rmrs) * R;        // 1 / sin
+  G.g_t_tr = 0.5 * rs * ifd;
+  G.g_r_tt = 0.5 * rs * rmrs * (G.ir * G.ir * G.ir);
+  G.g_r_thth = -rmrs;
+  G.g_r_phph = -rmrs * s * s;
+  G.g_th_phph = -s * c;
+  G.g_ph_thph = c * is;
+  return G;
+}
+
+GG_DEV void schw_contract(const SchwGeo& G, const double v[4], double a[4]) {
+  const double vt = v[0], vr = v[1], vth = v[2], vph = v[3];
+  a[0] = -2.0 * G.g_t_tr * vt * vr;
+  a[1] = -G.g_r_tt * vt * vt + G.g_t_tr * vr * vr - G.g_r_thth * vth * vth -
+         G.g_r_phph * vph * vph;
+  a[2] = -2.0 * G.ir * vr * vth - G.g_th_phph * vph * vph;
+  a[3] = -2.0 * G.ir * vr * vph - 2.0 * G.g_ph_thph * vth * vph;
 }
 
 template <int METRIC>
-GG_DEV void rhs(const DevParams& P, double r, double th, const double v[4], double a[4]) {
-  if (METRIC == kMetricKerr) {
-    rhs_kerr(P, r, th, v, a);
-  } else {
-    rhs_schwarzschild(P, r, th, v, a);
+struct Geometry;
+
+template <>
+struct Geometry<kMetricKerr> {
+  KerrGeo<double> g;
+  GG_DEV void at(const DevParams& P, double r, double th) {
+    double s, c;
+    sincos(th, &s, &c);
+    g = kerr_geometry<double>(P.mass, P.spin, fmax(r, 1e-10), s, c);
   }
+  GG_DEV void accel(const double v[4], double a[4]) const { kerr_contract<double>(g, v, a); }
+};
+
+template <>
+struct Geometry<kMetricSchwarzschild> {
+  SchwGeo g;
+  GG_DEV void at(const DevParams& P, double r, double th) {
+    double s, c;
+    sincos(th, &s, &c);
+    g = schw_geometry(P.rs, fmax(r, 1e-10), s, c);
+  }
+  GG_DEV void accel(const double v[4], double a[4]) const { schw_contract(g, v, a); }
+};
+
+template <int METRIC>
+GG_DEV void rhs(const DevParams& P, double r, double th, const double v[4], double a[4]) {
+  Geometry<METRIC> G;
+  G.at(P, r, th);
+  G.accel(v, a);
 }
 
 // ---------------------------------------------------------------------------
@@ -232,9 +268,39 @@ GG_DEV void normalize_coords(double x[4]) {
     x[2] = kTwoPi - x[2];
     x[3] = x[3] + kPi;
   }
-  double m = fmod(x[3], kTwoPi);
-  if (m < 0.0) m = m + kTwoPi;
+  // phi.rem_euclid(2 pi).  An accepted step moves phi by far less than 2 pi,
+  // so the fmod loop is only needed outside (-2 pi, 4 pi); inside, the result
+  // is the same number: on [2 pi, 4 pi) fmod returns p - 2 pi, which that
+  // subtraction produces exactly (Sterbenz); on (-2 pi, 0) fmod returns p.
+  const double p = x[3];
+  double m;
+  if (p >= 0.0 && p < kTwoPi) {
+    m = p;
+  } else if (p >= kTwoPi && p < 2.0 * kTwoPi) {
+    m = p - kTwoPi;
+  } else if (p < 0.0 && p > -kTwoPi) {
+    m = p + kTwoPi;
+  } else {
+    m = fmod(p, kTwoPi);
+    if (m < 0.0) m = m + kTwoPi;
+  }
   x[3] = m;
+}
+
+// x^(1/5) for the step-size law (geodesic.rs:318): a single-precision seed
+// refined by two Newton steps on z = x^(-1/5), z <- z (6/5 - x z^5 / 5),
+// which needs no division; x^(1/5) = x z^4.  Agrees with pow(x, 0.2) to a
+// few ulp on the range where the seed is representable, pow elsewhere.
+GG_DEV double fifth_root(double x) {
+  if (!(x >= 1e-30 && x <= 1e30)) return pow(x, 0.2);
+  double z = (double)__powf((float)x, -0.2f);
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const double z2 = z * z;
+    z = z * (1.2 - 0.2 * x * (z2 * z2 * z));
+  }
+  const double z2 = z * z;
+  return x * (z2 * z2);
 }
 
 // Dormand-Prince tableau (geodesic.rs:210-242).
@@ -264,6 +330,28 @@ GG_DEV bool stage_pos(const Ray& R, double ha, double& r, double& th) {
   return finite4(t, r, th, ph) && r > 0.0;
 }
 
+// v + h (c1 k1 + c3 k3 + c4 k4 + c5 k5 + c6 k6), left to right, uncontracted
+// (geodesic.rs:294-295).
+GG_DEV double combine5(double v, double h, double k1, double k3, double k4, double k5,
+                       double k6) {
+  double s = add_rn(mul_rn(DP::c1, k1), mul_rn(DP::c3, k3));
+  s = add_rn(s, mul_rn(DP::c4, k4));
+  s = add_rn(s, mul_rn(DP::c5, k5));
+  s = add_rn(s, mul_rn(DP::c6, k6));
+  return add_rn(v, mul_rn(h, s));
+}
+
+// v + h (d1 k1 + d3 k3 + d4 k4 + d5 k5 + d6 k6 + d7 k7), likewise (:299-305).
+GG_DEV double combine4(double v, double h, double k1, double k3, double k4, double k5,
+                       double k6, double k7) {
+  double s = add_rn(mul_rn(DP::d1, k1), mul_rn(DP::d3, k3));
+  s = add_rn(s, mul_rn(DP::d4, k4));
+  s = add_rn(s, mul_rn(DP::d5, k5));
+  s = add_rn(s, mul_rn(DP::d6, k6));
+  s = add_rn(s, mul_rn(DP::d7, k7));
+  return add_rn(v, mul_rn(h, s));
+}
+
 // One call of RK45Integrator::step (geodesic.rs:185-328) in FP64.
 // Returns the StepResult; `accepted` and `h_used` describe an advance.
 template <int METRIC>
@@ -273,89 +361,134 @@ GG_DEV int attempt_fp64(const DevParams& P, Ray& R, bool& accepted, double& h_us
   if (P.has_horizon && (R.x[1] < P.rh_plus_buffer || R.x[1] < P.rh)) return kHorizon;
 
   const double h = R.h;
-  double k1[4], k2[4], k3[4], k4[4], k5[4], k6[4], k7[4], w[4];
-  double r, th;
-  rhs<METRIC>(P, R.x[1], R.x[2], R.v, k1);
-
-  if (!stage_pos(R, h * DP::a2, r, th)) { R.h = h * 0.5; return kContinue; }
+  double k1[4], k2[4], k3[4], k4[4], k5[4], k6[4], k7[4], nv[4];
+  double r = R.x[1], th = R.x[2];
+  // The right-hand-side evaluations run as one loop so the RHS code (sincos,
+  // reciprocal, ~150 FP64 ops) is emitted once: unrolled, seven copies
+  // overflow the instruction cache and warps stall on fetch.  The stage
+  // inputs and the k registers are selected per stage by switch arms
+  // (warp-uniform branches; all lanes of a warp run the same stage).  The
+  // last pass evaluates k6 and k7, which share the position pos6.
+#pragma unroll 1
+  for (int s = 0; s < 6; ++s) {
+    double w[4];
+    switch (s) {
+      case 0:
 #pragma unroll
-  for (int i = 0; i < 4; ++i) w[i] = R.v[i] + (h * DP::b21) * k1[i];
-  rhs<METRIC>(P, r, th, w, k2);
-
-  if (!stage_pos(R, h * DP::a3, r, th)) { R.h = h * 0.5; return kContinue; }
+        for (int i = 0; i < 4; ++i) w[i] = R.v[i];
+        break;
+      case 1:
+        if (!stage_pos(R, h * DP::a2, r, th)) { R.h = h * 0.5; return kContinue; }
 #pragma unroll
-  for (int i = 0; i < 4; ++i) w[i] = R.v[i] + h * (DP::b31 * k1[i] + DP::b32 * k2[i]);
-  rhs<METRIC>(P, r, th, w, k3);
-
-  if (!stage_pos(R, h * DP::a4, r, th)) { R.h = h * 0.5; return kContinue; }
+        for (int i = 0; i < 4; ++i) w[i] = R.v[i] + (h * DP::b21) * k1[i];
+        break;
+      case 2:
+        if (!stage_pos(R, h * DP::a3, r, th)) { R.h = h * 0.5; return kContinue; }
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
-    w[i] = R.v[i] + h * (DP::b41 * k1[i] + DP::b42 * k2[i] + DP::b43 * k3[i]);
-  rhs<METRIC>(P, r, th, w, k4);
-
-  if (!stage_pos(R, h * DP::a5, r, th)) { R.h = h * 0.5; return kContinue; }
+        for (int i = 0; i < 4; ++i) w[i] = R.v[i] + h * (DP::b31 * k1[i] + DP::b32 * k2[i]);
+        break;
+      case 3:
+        if (!stage_pos(R, h * DP::a4, r, th)) { R.h = h * 0.5; return kContinue; }
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
-    w[i] = R.v[i] +
-           h * (DP::b51 * k1[i] + DP::b52 * k2[i] + DP::b53 * k3[i] + DP::b54 * k4[i]);
-  rhs<METRIC>(P, r, th, w, k5);
-
-  if (!stage_pos(R, h, r, th)) { R.h = h * 0.5; return kContinue; }
+        for (int i = 0; i < 4; ++i)
+          w[i] = R.v[i] + h * (DP::b41 * k1[i] + DP::b42 * k2[i] + DP::b43 * k3[i]);
+        break;
+      case 4:
+        if (!stage_pos(R, h * DP::a5, r, th)) { R.h = h * 0.5; return kContinue; }
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
-    w[i] = R.v[i] + h * (DP::b61 * k1[i] + DP::b62 * k2[i] + DP::b63 * k3[i] +
-                         DP::b64 * k4[i] + DP::b65 * k5[i]);
-  rhs<METRIC>(P, r, th, w, k6);
-
-  double nv[4];
+        for (int i = 0; i < 4; ++i)
+          w[i] = R.v[i] +
+                 h * (DP::b51 * k1[i] + DP::b52 * k2[i] + DP::b53 * k3[i] + DP::b54 * k4[i]);
+        break;
+      default:
+        if (!stage_pos(R, h, r, th)) { R.h = h * 0.5; return kContinue; }
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
-    nv[i] = R.v[i] + h * (DP::c1 * k1[i] + DP::c3 * k3[i] + DP::c4 * k4[i] + DP::c5 * k5[i] +
-                          DP::c6 * k6[i]);
-  rhs<METRIC>(P, r, th, nv, k7);
+        for (int i = 0; i < 4; ++i)
+          w[i] = R.v[i] + h * (DP::b61 * k1[i] + DP::b62 * k2[i] + DP::b63 * k3[i] +
+                               DP::b64 * k4[i] + DP::b65 * k5[i]);
+        break;
+    }
+    Geometry<METRIC> G;
+    G.at(P, r, th);
+    double a[4];
+    G.accel(w, a);
+    switch (s) {
+      case 0:
+#pragma unroll
+        for (int i = 0; i < 4; ++i) k1[i] = a[i];
+        break;
+      case 1:
+#pragma unroll
+        for (int i = 0; i < 4; ++i) k2[i] = a[i];
+        break;
+      case 2:
+#pragma unroll
+        for (int i = 0; i < 4; ++i) k3[i] = a[i];
+        break;
+      case 3:
+#pragma unroll
+        for (int i = 0; i < 4; ++i) k4[i] = a[i];
+        break;
+      case 4:
+#pragma unroll
+        for (int i = 0; i < 4; ++i) k5[i] = a[i];
+        break;
+      default:
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          k6[i] = a[i];
+          nv[i] = combine5(R.v[i], h, k1[i], k3[i], k4[i], k5[i], k6[i]);
+        }
+        G.accel(nv, k7);  // k7 at (pos6, new_vel), geodesic.rs:298
+        break;
+    }
+  }
 
+  // err = |new_vel - vel_err| (geodesic.rs:299-308).  The two vectors agree
+  // to ~tol, so err is their last few bits: both are formed exactly as the
+  // reference groups them, without fused multiply-adds, so that only the
+  // (much smaller) differences in the k's reach the step-size law.
   double err, tol;
   if (P.rtol > 0.0) {
     double ssum = 0.0;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-      const double ve = R.v[i] + h * (DP::d1 * k1[i] + DP::d3 * k3[i] + DP::d4 * k4[i] +
-                                      DP::d5 * k5[i] + DP::d6 * k6[i] + DP::d7 * k7[i]);
-      const double sc = P.atol + P.rtol * fmax(fabs(R.v[i]), fabs(nv[i]));
-      const double q = (nv[i] - ve) / sc;
-      ssum = ssum + q * q;
+      const double ve = combine4(R.v[i], h, k1[i], k3[i], k4[i], k5[i], k6[i], k7[i]);
+      const double sc = add_rn(P.atol, mul_rn(P.rtol, fmax(fabs(R.v[i]), fabs(nv[i]))));
+      const double q = __ddiv_rn(sub_rn(nv[i], ve), sc);
+      ssum = add_rn(ssum, mul_rn(q, q));
     }
-    err = sqrt(ssum * 0.25);
+    err = __dsqrt_rn(mul_rn(ssum, 0.25));
     tol = 1.0;
   } else {
     double ssum = 0.0;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-      const double ve = R.v[i] + h * (DP::d1 * k1[i] + DP::d3 * k3[i] + DP::d4 * k4[i] +
-                                      DP::d5 * k5[i] + DP::d6 * k6[i] + DP::d7 * k7[i]);
-      const double d = nv[i] - ve;
-      ssum = ssum + d * d;
+      const double ve = combine4(R.v[i], h, k1[i], k3[i], k4[i], k5[i], k6[i], k7[i]);
+      const double d = sub_rn(nv[i], ve);
+      ssum = add_rn(ssum, mul_rn(d, d));
     }
-    err = sqrt(ssum);
+    err = __dsqrt_rn(ssum);
     tol = P.tolerance;
   }
 
   if (err < tol || h <= P.min_step) {
 #pragma unroll
-    for (int i = 0; i < 4; ++i) R.x[i] = R.x[i] + h * R.v[i];
+    for (int i = 0; i < 4; ++i) R.x[i] = add_rn(R.x[i], mul_rn(h, R.v[i]));  // geodesic.rs:312
 #pragma unroll
     for (int i = 0; i < 4; ++i) R.v[i] = nv[i];
-    R.lam = R.lam + h;
+    R.lam = add_rn(R.lam, h);
     normalize_coords(R.x);
     accepted = true;
     h_used = h;
     if (err > 0.0) {
-      double hn = h * 0.9 * pow(tol / err, 0.2);
+      double hn = h * 0.9 * fifth_root(tol / err);
       hn = hn < P.min_step ? P.min_step : (hn > P.max_step ? P.max_step : hn);
       R.h = hn;
     }
   } else {
-    R.h = fmax(h * 0.9 * pow(tol / err, 0.25), P.min_step);
+    // (tol/err)^0.25 as two correctly rounded square roots
+    R.h = fmax(h * 0.9 * sqrt(sqrt(tol / err)), P.min_step);
   }
   return kContinue;
 }

@@ -22,7 +22,10 @@ namespace gg {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
-constexpr int kPeriod = 2;     // attempts between refills
+#ifndef GG_TRACE_PERIOD
+#define GG_TRACE_PERIOD 4
+#endif
+constexpr int kPeriod = GG_TRACE_PERIOD;  // attempts between refills
 constexpr uint32_t kChunk = 32;  // samples a warp takes from the queue at once
 
 GG_DEV unsigned lanemask_lt() {
@@ -108,7 +111,7 @@ GG_DEV void store_cross(const DevParams& P, const DevOutputs& O, uint64_t idx,
 }
 
 template <int METRIC, int DISK>
-__global__ void __launch_bounds__(kTraceBlock)
+__global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks)
     trace_fp64_kernel(const __grid_constant__ DevParams P, const __grid_constant__ DevOutputs O,
                       DevControl* ctl) {
   const unsigned lane = threadIdx.x & 31u;

@@ -235,12 +235,28 @@ class Renderer:
         abi.check(st, "gg_render")
         return img, out
 
+    def render_into(self, scene: Scene, rgb_host: np.ndarray) -> None:
+        """Synchronous render into a caller-owned (e.g. pinned) uint8 host buffer."""
+        assert rgb_host.dtype == np.uint8 and rgb_host.size >= scene.width * scene.height * 3
+        st = self._lib.gg_render(self._h, *scene.c_args(), rgb_host.ctypes.data_as(C.c_void_p),
+                                 None)
+        abi.check(st, "gg_render")
+
+    def fma_peak(self, fp64: bool = True) -> float:
+        """Measured FMA throughput of this device in FLOP/s."""
+        f = C.c_double()
+        abi.check(self._lib.gg_measure_fma_peak(self._h, 1 if fp64 else 0, C.byref(f)),
+                  "gg_measure_fma_peak")
+        return f.value
+
     def render_device(self, scene: Scene, rgb_dev: int, rays_dev: abi.gg_ray_out_t | None = None,
                       stream: int | None = None) -> None:
-        """Enqueue a render writing device pointers (no synchronisation)."""
+        """Enqueue a render writing device pointers (no synchronisation).
+
+        ``stream`` is a cudaStream_t handle; None or 0 is CUDA's default stream."""
         st = self._lib.gg_render_device(self._h, *scene.c_args(), C.c_void_p(rgb_dev),
                                         C.byref(rays_dev) if rays_dev is not None else None,
-                                        C.c_void_p(stream) if stream else None)
+                                        C.c_void_p(stream or 0))
         abi.check(st, "gg_render_device")
 
     def stats(self) -> abi.gg_stats_t:

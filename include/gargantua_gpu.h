@@ -204,12 +204,20 @@ GG_API int gg_render(gg_ctx* ctx, const gg_metric_t* metric, const gg_camera_t* 
                      uint8_t* rgb_out, const gg_ray_out_t* rays_out);
 
 /* Same render with DEVICE output pointers, enqueued on `stream` (a
- * cudaStream_t; NULL = the context's stream) without synchronising.
- * Scratch comes from the context. */
+ * cudaStream_t; NULL is CUDA's default stream; gg_stream(ctx) gives the
+ * context's own) without synchronising.  Scratch comes from the context;
+ * gg_last_stats waits for this render. */
 GG_API int gg_render_device(gg_ctx* ctx, const gg_metric_t* metric, const gg_camera_t* camera,
                             const gg_disk_t* disk, const gg_integrator_t* integ,
                             const gg_render_opts_t* opts, uint32_t width, uint32_t height,
                             uint8_t* rgb_dev, const gg_ray_out_t* rays_dev, void* stream);
+
+/* ---- measurement ------------------------------------------------------- */
+/* FMA throughput of the context's device in FLOP/s (an FMA counts 2), best
+ * of 5 timed launches of independent FMA chains: fp64 = 1 for the FP64 pipe,
+ * 0 for FP32.  The roofline denominator of the trace kernels.  No reference
+ * counterpart (the reference has no device code). */
+GG_API int gg_measure_fma_peak(gg_ctx* ctx, int fp64, double* flops);
 
 #ifdef __cplusplus
 }

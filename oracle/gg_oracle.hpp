@@ -332,6 +332,15 @@ struct Kerr {
   // contracts the dense Christoffel array in mu, alpha, beta order.
   template <class T>
   V4<T> geodesic_acceleration(const V4<T>& pos, const V4<T>& vel) const {
+#ifdef GGO_ALT_KERR_RHS
+    // NOT the reference formulation.  Built only into liboracle_gg_alt.so,
+    // whose deviation from the plain build measures how much each ray's
+    // endpoint moves when the same right-hand side is rounded through a
+    // different (algebraically equivalent) arrangement: the 20 non-zero
+    // symbols folded into the contraction, one reciprocal for 1/Sigma,
+    // 1/Delta, 1/sin^2.
+    return alt_acceleration(pos, vel);
+#endif
     T gamma[4][4][4];
     christoffel(pos, gamma);
     V4<T> acc{{T(0.0), T(0.0), T(0.0), T(0.0)}};
@@ -340,6 +349,43 @@ struct Kerr {
         for (int beta = 0; beta < 4; ++beta)
           acc[mu] = acc[mu] - gamma[mu][alpha][beta] * vel[alpha] * vel[beta];
     return acc;
+  }
+
+  template <class T>
+  V4<T> alt_acceleration(const V4<T>& pos, const V4<T>& vel) const {
+    using std::cos;
+    using std::sin;
+    const T r = rmax(pos[1], T(1e-10));
+    const T s = sin(pos[2]), c = cos(pos[2]);
+    const T M(mass), a(spin);
+    const T r2 = r * r, a2 = a * a, s2 = s * s, c2 = c * c, sc = s * c;
+    const T sig = r2 + a2 * c2, del = (r - T(2) * M) * r + a2, rho = r2 + a2, sd = sig * del;
+    const T R = T(1) / (sd * s2);
+    const T iSD = s2 * R, iS = del * iSD, iD = sig * iSD, is2 = sd * R, iS2 = iS * iS;
+    const T Mr = M * r, sm2r = a2 * c2 - r2;
+    const T dtt_r = T(2) * M * sm2r * iS2, dtt_th = T(4) * Mr * a2 * sc * iS2;
+    const T drr_r = T(2) * (a2 * (r * s2 + M * c2) - M * r2) * (iD * iD);
+    const T drr_th = T(-2) * a2 * sc * iD;
+    const T dthth_r = T(2) * r, dthth_th = T(-2) * a2 * sc;
+    const T dphph_r = T(2) * r * s2 + T(2) * M * a2 * (s2 * s2) * sm2r * iS2;
+    const T dphph_th = T(2) * rho * sc + T(4) * Mr * a2 * sc * s2 * (sig + rho) * iS2;
+    const T dtph_r = T(-2) * M * a * s2 * sm2r * iS2, dtph_th = T(-4) * Mr * a * sc * rho * iS2;
+    const T gtt = -(rho * rho - a2 * del * s2) * iSD, gtph = T(-2) * Mr * a * iSD;
+    const T gphph = (del - a2 * s2) * iSD * is2;
+    const T vt = vel[0], vr = vel[1], vth = vel[2], vph = vel[3];
+    const T Et = vr * (dtt_r * vt + dtph_r * vph) + vth * (dtt_th * vt + dtph_th * vph);
+    const T Ep = vr * (dtph_r * vt + dphph_r * vph) + vth * (dtph_th * vt + dphph_th * vph);
+    const T two_tp = T(2) * vt * vph, two_rt = T(2) * vr * vth;
+    V4<T> out;
+    out[0] = -(gtt * Et + gtph * Ep);
+    out[3] = -(gtph * Et + gphph * Ep);
+    out[1] = T(-0.5) * del * iS *
+             (drr_r * vr * vr - dtt_r * vt * vt - dthth_r * vth * vth - dphph_r * vph * vph +
+              drr_th * two_rt - dtph_r * two_tp);
+    out[2] = T(-0.5) * iS *
+             (dthth_th * vth * vth - dtt_th * vt * vt - drr_th * vr * vr - dphph_th * vph * vph +
+              dthth_r * two_rt - dtph_th * two_tp);
+    return out;
   }
 
   bool event_horizon(double* rh) const {  // :427-436

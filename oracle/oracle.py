@@ -27,15 +27,23 @@ def build() -> Path:
     return LIB_PATH
 
 
-_LIB = None
+VARIANT_PATHS = {
+    "plain": LIB_PATH,
+    # same algorithm rounded differently; used only to measure each ray's
+    # sensitivity to last-bit rounding, never as the reference
+    "fma": ORACLE_DIR / "_build" / "liboracle_gg_fma.so",
+    "alt": ORACLE_DIR / "_build" / "liboracle_gg_alt.so",
+}
+_LIBS: dict = {}
 
 
-def lib() -> C.CDLL:
-    global _LIB
-    if _LIB is None:
-        if not LIB_PATH.exists():
+def lib(variant: str = "plain") -> C.CDLL:
+    """The oracle library, or one of its rounding-perturbed builds."""
+    path = VARIANT_PATHS[variant]
+    if path not in _LIBS:
+        if not path.exists():
             build()
-        L = C.CDLL(str(LIB_PATH))
+        L = C.CDLL(str(path))
         common = [P(abi.gg_metric_t), P(abi.gg_camera_t), P(abi.gg_disk_t),
                   P(abi.gg_integrator_t), P(abi.gg_render_opts_t), C.c_uint32, C.c_uint32]
         sig = {
@@ -83,8 +91,8 @@ def lib() -> C.CDLL:
             f = getattr(L, name)
             f.restype = res
             f.argtypes = args
-        _LIB = L
-    return _LIB
+        _LIBS[path] = L
+    return _LIBS[path]
 
 
 def _ptr(a: np.ndarray):
@@ -94,7 +102,7 @@ def _ptr(a: np.ndarray):
 from gargantua_b200.curved import RayOutputs as RayArrays  # noqa: E402
 
 
-def render(scene, threads: int = 0, rays: bool = True):
+def render(scene, threads: int = 0, rays: bool = True, variant: str = "plain"):
     """Render ``scene`` (a ``gargantua_b200.curved.Scene``) on the CPU oracle.
 
     Returns (rgb uint8 [H, W, 3], RayArrays or None)."""
@@ -102,16 +110,17 @@ def render(scene, threads: int = 0, rays: bool = True):
     n = w * h * scene.spp
     img = np.zeros((h, w, 3), np.uint8)
     ra = RayArrays(n) if rays else None
-    st = lib().ggo_render(*scene.c_args(), _ptr(img), C.byref(ra.struct()) if ra else None,
+    st = lib(variant).ggo_render(*scene.c_args(), _ptr(img), C.byref(ra.struct()) if ra else None,
                           threads)
     abi.check(st, "ggo_render")
     return img, ra
 
 
-def trace_samples(scene, index: np.ndarray, threads: int = 0) -> RayArrays:
+def trace_samples(scene, index: np.ndarray, threads: int = 0,
+                  variant: str = "plain") -> RayArrays:
     index = np.ascontiguousarray(index, np.uint64)
     ra = RayArrays(len(index))
-    st = lib().ggo_trace_samples(*scene.c_args(), _ptr(index), len(index),
+    st = lib(variant).ggo_trace_samples(*scene.c_args(), _ptr(index), len(index),
                                  C.byref(ra.struct()), threads)
     abi.check(st, "ggo_trace_samples")
     return ra
