@@ -18,6 +18,7 @@
 
 #include <cstdint>
 
+#include "gg_launch.h"
 #include "gg_params.h"
 
 namespace gg {
@@ -330,6 +331,25 @@ GG_DEV bool stage_pos(const Ray& R, double ha, double& r, double& th) {
   return finite4(t, r, th, ph) && r > 0.0;
 }
 
+// Where the stage derivatives k1..k6 live between the stages of an attempt:
+// registers, or (GG_K_SHARED) this thread's column of a block-shared array,
+// [stage][component][thread] so a warp's accesses are conflict-free.  The
+// shared form frees 48 registers of the stepping loop for occupancy.
+#ifndef GG_K_SHARED
+#define GG_K_SHARED 1
+#endif
+#if GG_K_SHARED
+struct KStore {
+  double (*s)[4][kTraceBlock];
+  GG_DEV double& operator()(int stage, int i) const { return s[stage][i][threadIdx.x]; }
+};
+#else
+struct KStore {
+  double k[6][4];
+  GG_DEV double& operator()(int stage, int i) { return k[stage][i]; }
+};
+#endif
+
 // v + h (c1 k1 + c3 k3 + c4 k4 + c5 k5 + c6 k6), left to right, uncontracted
 // (geodesic.rs:294-295).
 GG_DEV double combine5(double v, double h, double k1, double k3, double k4, double k5,
@@ -361,7 +381,13 @@ GG_DEV int attempt_fp64(const DevParams& P, Ray& R, bool& accepted, double& h_us
   if (P.has_horizon && (R.x[1] < P.rh_plus_buffer || R.x[1] < P.rh)) return kHorizon;
 
   const double h = R.h;
-  double k1[4], k2[4], k3[4], k4[4], k5[4], k6[4], k7[4], nv[4];
+#if GG_K_SHARED
+  __shared__ double k_smem[6][4][kTraceBlock];
+  KStore K{k_smem};
+#else
+  KStore K;
+#endif
+  double k7[4], nv[4];
   double r = R.x[1], th = R.x[2];
   // The right-hand-side evaluations run as one loop so the RHS code (sincos,
   // reciprocal, ~150 FP64 ops) is emitted once: unrolled, seven copies
@@ -380,32 +406,32 @@ GG_DEV int attempt_fp64(const DevParams& P, Ray& R, bool& accepted, double& h_us
       case 1:
         if (!stage_pos(R, h * DP::a2, r, th)) { R.h = h * 0.5; return kContinue; }
 #pragma unroll
-        for (int i = 0; i < 4; ++i) w[i] = R.v[i] + (h * DP::b21) * k1[i];
+        for (int i = 0; i < 4; ++i) w[i] = R.v[i] + (h * DP::b21) * K(0, i);
         break;
       case 2:
         if (!stage_pos(R, h * DP::a3, r, th)) { R.h = h * 0.5; return kContinue; }
 #pragma unroll
-        for (int i = 0; i < 4; ++i) w[i] = R.v[i] + h * (DP::b31 * k1[i] + DP::b32 * k2[i]);
+        for (int i = 0; i < 4; ++i) w[i] = R.v[i] + h * (DP::b31 * K(0, i) + DP::b32 * K(1, i));
         break;
       case 3:
         if (!stage_pos(R, h * DP::a4, r, th)) { R.h = h * 0.5; return kContinue; }
 #pragma unroll
         for (int i = 0; i < 4; ++i)
-          w[i] = R.v[i] + h * (DP::b41 * k1[i] + DP::b42 * k2[i] + DP::b43 * k3[i]);
+          w[i] = R.v[i] + h * (DP::b41 * K(0, i) + DP::b42 * K(1, i) + DP::b43 * K(2, i));
         break;
       case 4:
         if (!stage_pos(R, h * DP::a5, r, th)) { R.h = h * 0.5; return kContinue; }
 #pragma unroll
         for (int i = 0; i < 4; ++i)
           w[i] = R.v[i] +
-                 h * (DP::b51 * k1[i] + DP::b52 * k2[i] + DP::b53 * k3[i] + DP::b54 * k4[i]);
+                 h * (DP::b51 * K(0, i) + DP::b52 * K(1, i) + DP::b53 * K(2, i) + DP::b54 * K(3, i));
         break;
       default:
         if (!stage_pos(R, h, r, th)) { R.h = h * 0.5; return kContinue; }
 #pragma unroll
         for (int i = 0; i < 4; ++i)
-          w[i] = R.v[i] + h * (DP::b61 * k1[i] + DP::b62 * k2[i] + DP::b63 * k3[i] +
-                               DP::b64 * k4[i] + DP::b65 * k5[i]);
+          w[i] = R.v[i] + h * (DP::b61 * K(0, i) + DP::b62 * K(1, i) + DP::b63 * K(2, i) +
+                               DP::b64 * K(3, i) + DP::b65 * K(4, i));
         break;
     }
     Geometry<METRIC> G;
@@ -415,29 +441,29 @@ GG_DEV int attempt_fp64(const DevParams& P, Ray& R, bool& accepted, double& h_us
     switch (s) {
       case 0:
 #pragma unroll
-        for (int i = 0; i < 4; ++i) k1[i] = a[i];
+        for (int i = 0; i < 4; ++i) K(0, i) = a[i];
         break;
       case 1:
 #pragma unroll
-        for (int i = 0; i < 4; ++i) k2[i] = a[i];
+        for (int i = 0; i < 4; ++i) K(1, i) = a[i];
         break;
       case 2:
 #pragma unroll
-        for (int i = 0; i < 4; ++i) k3[i] = a[i];
+        for (int i = 0; i < 4; ++i) K(2, i) = a[i];
         break;
       case 3:
 #pragma unroll
-        for (int i = 0; i < 4; ++i) k4[i] = a[i];
+        for (int i = 0; i < 4; ++i) K(3, i) = a[i];
         break;
       case 4:
 #pragma unroll
-        for (int i = 0; i < 4; ++i) k5[i] = a[i];
+        for (int i = 0; i < 4; ++i) K(4, i) = a[i];
         break;
       default:
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-          k6[i] = a[i];
-          nv[i] = combine5(R.v[i], h, k1[i], k3[i], k4[i], k5[i], k6[i]);
+          K(5, i) = a[i];
+          nv[i] = combine5(R.v[i], h, K(0, i), K(2, i), K(3, i), K(4, i), K(5, i));
         }
         G.accel(nv, k7);  // k7 at (pos6, new_vel), geodesic.rs:298
         break;
@@ -453,7 +479,7 @@ GG_DEV int attempt_fp64(const DevParams& P, Ray& R, bool& accepted, double& h_us
     double ssum = 0.0;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-      const double ve = combine4(R.v[i], h, k1[i], k3[i], k4[i], k5[i], k6[i], k7[i]);
+      const double ve = combine4(R.v[i], h, K(0, i), K(2, i), K(3, i), K(4, i), K(5, i), k7[i]);
       const double sc = add_rn(P.atol, mul_rn(P.rtol, fmax(fabs(R.v[i]), fabs(nv[i]))));
       const double q = __ddiv_rn(sub_rn(nv[i], ve), sc);
       ssum = add_rn(ssum, mul_rn(q, q));
@@ -464,7 +490,7 @@ GG_DEV int attempt_fp64(const DevParams& P, Ray& R, bool& accepted, double& h_us
     double ssum = 0.0;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-      const double ve = combine4(R.v[i], h, k1[i], k3[i], k4[i], k5[i], k6[i], k7[i]);
+      const double ve = combine4(R.v[i], h, K(0, i), K(2, i), K(3, i), K(4, i), K(5, i), k7[i]);
       const double d = sub_rn(nv[i], ve);
       ssum = add_rn(ssum, mul_rn(d, d));
     }

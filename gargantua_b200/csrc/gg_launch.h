@@ -7,14 +7,21 @@
 
 namespace gg {
 
-#ifndef GG_TRACE_MIN_BLOCKS
-#define GG_TRACE_MIN_BLOCKS 4
-#endif
-
 constexpr int kTraceBlock = 128;  // threads per CTA of the trace kernels
-// resident CTAs per SM the register budget targets (65536 / (128 * 4) = 128
-// registers; the few spills this forces cost less than the extra warps gain)
-constexpr int kTraceMinBlocks = GG_TRACE_MIN_BLOCKS;
+
+// Resident CTAs per SM each metric's trace kernel is register-budgeted for
+// (65536 / (128 * blocks) registers per thread).  Kerr's stepping loop hides
+// FP64 latency better with 6 CTAs (80 registers, k vectors in shared
+// memory) despite a few spills; Schwarzschild's lighter right-hand side is
+// fastest at 4.  Measured on B200, Kerr 1920x1080: 4 -> 53.8 ms, 5 -> 50.9
+// ms, 6 -> 49.2 ms.  GG_TRACE_MIN_BLOCKS overrides both (tuning builds).
+#ifdef GG_TRACE_MIN_BLOCKS
+constexpr int kTraceMinBlocksKerr = GG_TRACE_MIN_BLOCKS;
+constexpr int kTraceMinBlocksSchw = GG_TRACE_MIN_BLOCKS;
+#else
+constexpr int kTraceMinBlocksKerr = 6;
+constexpr int kTraceMinBlocksSchw = 4;
+#endif
 
 // Resident CTAs per SM of the trace kernel `P` selects.
 cudaError_t trace_occupancy(const DevParams& P, int* blocks_per_sm);

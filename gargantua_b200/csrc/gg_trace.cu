@@ -34,13 +34,13 @@ GG_DEV unsigned lanemask_lt() {
   return m;
 }
 
-// Writes the finished sample's outcome and colour.
-struct Finisher {
-  const DevParams& P;
-  const DevOutputs& O;
-
-  GG_DEV void operator()(uint64_t idx, int cls, const Ray& R, uint32_t n_att, uint32_t n_acc,
-                         double intensity, double color_temp, bool crossed) const {
+// Writes the finished sample's outcome and colour.  Runs once per ray, so it
+// is kept out of line: its shading code (several pow) would otherwise sit in
+// the hot stepping loop's instruction footprint.
+__device__ __noinline__ void finish_sample(const DevParams& P, const DevOutputs& O, uint64_t idx,
+                                           int cls, Ray R, uint32_t n_att, uint32_t n_acc,
+                                           double intensity, double color_temp, bool crossed) {
+  {
     const uint64_t n = P.n_rays;
     double lin[3];
     if (cls == kClsHorizon || cls == kClsBudget) {
@@ -88,6 +88,22 @@ struct Finisher {
       for (int c = 0; c < 3; ++c) O.rgb8[3 * idx + c] = encode_channel(lin[c]);
     }
   }
+}
+
+// Camera ray of sample idx (once per ray, out of line like finish_sample).
+__device__ __noinline__ Ray start_sample(const DevParams& P, uint64_t idx) {
+  double u, v;
+  sample_uv(P, idx, u, v);
+  Ray R;
+  init_ray(P, u, v, R);
+  return R;
+}
+
+// Per-block totals of the statistics (one shared-memory atomic per finished
+// ray instead of per-thread counters, which would cost registers in the
+// stepping loop); flushed to DevControl when the block exits.
+struct BlockStats {
+  unsigned long long attempts, accepted, cls[5];
 };
 
 // Point at fraction s of the last accepted Euler segment (the reference moves
@@ -111,11 +127,22 @@ GG_DEV void store_cross(const DevParams& P, const DevOutputs& O, uint64_t idx,
 }
 
 template <int METRIC, int DISK>
-__global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks)
+__global__ void __launch_bounds__(kTraceBlock,
+                                  METRIC == kMetricKerr ? kTraceMinBlocksKerr : kTraceMinBlocksSchw)
     trace_fp64_kernel(const __grid_constant__ DevParams P, const __grid_constant__ DevOutputs O,
                       DevControl* ctl) {
   const unsigned lane = threadIdx.x & 31u;
-  const Finisher finish{P, O};
+  __shared__ BlockStats bs;
+  if (threadIdx.x < sizeof(BlockStats) / 8)
+    reinterpret_cast<unsigned long long*>(&bs)[threadIdx.x] = 0ull;
+  __syncthreads();
+  auto finish = [&](uint64_t i, int cls, const Ray& r, uint32_t na, uint32_t nc, double inten_o,
+                    double temp_o, bool cr) {
+    finish_sample(P, O, i, cls, r, na, nc, inten_o, temp_o, cr);
+    atomicAdd(&bs.attempts, (unsigned long long)na);
+    atomicAdd(&bs.accepted, (unsigned long long)nc);
+    atomicAdd(&bs.cls[cls], 1ull);
+  };
 
   Ray R;
   uint64_t idx = 0;
@@ -127,8 +154,7 @@ __global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks)
   uint64_t wbase = 0;
   uint32_t wcount = 0;
   bool wdone = false;
-  unsigned long long sum_att = 0, sum_acc = 0, budget_pending = 0;
-  uint32_t cls_count[5] = {0, 0, 0, 0, 0};
+  unsigned budget_pending = 0;
 
   for (;;) {
     // ---- refill lanes whose ray finished ----------------------------------
@@ -165,9 +191,7 @@ __global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks)
       const unsigned rank = (unsigned)__popc(need & lanemask_lt());
       if (!live && rank < take) {
         idx = wbase + rank;
-        double u, v;
-        sample_uv(P, idx, u, v);
-        init_ray(P, u, v, R);
+        R = start_sample(P, idx);
         live = true;
         n_att = 0;
         n_acc = 0;
@@ -295,16 +319,13 @@ __global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks)
       }
       if (done_cls >= 0) {
         finish(idx, done_cls, R, n_att, n_acc, out_int, out_temp, crossed);
-        cls_count[done_cls] += 1;
-        sum_att += n_att;
-        sum_acc += n_acc;
         budget_pending += n_att;
         live = false;
       }
     }
     if (P.attempt_budget) {
       // account finished work; stop live rays once the budget is gone
-      const unsigned long long wsum = __reduce_add_sync(kFull, (unsigned)budget_pending);
+      const unsigned long long wsum = __reduce_add_sync(kFull, budget_pending);
       budget_pending = 0;
       unsigned ab = 0;
       if (lane == 0) {
@@ -316,31 +337,20 @@ __global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks)
         wdone = true;
         if (live) {
           finish(idx, kClsBudget, R, n_att, n_acc, 0.0, 0.0, crossed);
-          cls_count[kClsBudget] += 1;
-          sum_att += n_att;
-          sum_acc += n_acc;
           live = false;
         }
       }
     }
   }
 
-  // ---- per-warp statistics ------------------------------------------------
-  unsigned long long wa = sum_att, wc = sum_acc;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    wa += __shfl_xor_sync(kFull, wa, o);
-    wc += __shfl_xor_sync(kFull, wc, o);
-  }
-  uint32_t cc[5];
-#pragma unroll
-  for (int k = 0; k < 5; ++k) cc[k] = __reduce_add_sync(kFull, cls_count[k]);
-  if (lane == 0) {
-    atomicAdd(&ctl->attempts, wa);
-    atomicAdd(&ctl->accepted, wc);
+  // ---- per-block statistics -----------------------------------------------
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    atomicAdd(&ctl->attempts, bs.attempts);
+    atomicAdd(&ctl->accepted, bs.accepted);
 #pragma unroll
     for (int k = 0; k < 5; ++k)
-      if (cc[k]) atomicAdd(&ctl->class_count[k], (unsigned long long)cc[k]);
+      if (bs.cls[k]) atomicAdd(&ctl->class_count[k], bs.cls[k]);
   }
 }
 
