@@ -24,6 +24,7 @@ GG_ERR_OOM = -3
 GG_ERR_BUDGET = -4
 GG_ERR_UNSUPPORTED = -5
 GG_ERR_NO_DEVICE = -6
+GG_ERR_TOO_LARGE = -7
 
 GG_METRIC_SCHWARZSCHILD = 0
 GG_METRIC_KERR = 1
@@ -125,6 +126,10 @@ _SIGNATURES = {
                                    P(gg_integrator_t), P(gg_render_opts_t), C.c_uint32,
                                    C.c_uint32, C.c_void_p, P(gg_ray_out_t), C.c_void_p]),
     "gg_measure_fma_peak": (C.c_int, [C.c_void_p, C.c_int, P(C.c_double)]),
+    "gg_render_device_noalloc": (C.c_int, [P(gg_metric_t), P(gg_camera_t), P(gg_disk_t),
+                                           P(gg_integrator_t), P(gg_render_opts_t), C.c_uint32,
+                                           C.c_uint32, C.c_void_p, P(gg_ray_out_t),
+                                           C.c_void_p]),
 }
 
 

@@ -14,6 +14,7 @@
 #include <new>
 
 #include "../../include/gargantua_gpu.h"
+#include "gg_host.h"
 #include "gg_launch.h"
 #include "gg_params.h"
 
@@ -336,6 +337,22 @@ struct Lock {
 
 }  // namespace
 
+namespace gg {
+
+int validate_render(const gg_metric_t* metric, const gg_camera_t* camera, const gg_disk_t* disk,
+                    const gg_integrator_t* integ, const gg_render_opts_t* opts, uint32_t width,
+                    uint32_t height) {
+  return validate(metric, camera, disk, integ, opts, width, height);
+}
+
+void make_params(const gg_metric_t* metric, const gg_camera_t* camera, const gg_disk_t* disk,
+                 const gg_integrator_t* integ, const gg_render_opts_t* opts, uint32_t width,
+                 uint32_t height, DevParams* out) {
+  build_params(metric, camera, disk, integ, opts, width, height, out);
+}
+
+}  // namespace gg
+
 extern "C" {
 
 GG_API const char* gg_version(void) { return "gargantua_b200 0.1.0 (sm_100a)"; }
@@ -349,6 +366,7 @@ GG_API const char* gg_strerror(int status) {
     case GG_ERR_BUDGET: return "attempt budget exhausted";
     case GG_ERR_UNSUPPORTED: return "unsupported combination";
     case GG_ERR_NO_DEVICE: return "no sm_100 CUDA device";
+    case GG_ERR_TOO_LARGE: return "render exceeds the fixed no-allocation scratch";
     default: return "unknown status";
   }
 }

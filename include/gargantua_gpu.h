@@ -48,6 +48,7 @@ extern "C" {
 #define GG_ERR_BUDGET (-4)      /* the attempt budget ran out mid-render   */
 #define GG_ERR_UNSUPPORTED (-5) /* combination not implemented             */
 #define GG_ERR_NO_DEVICE (-6)   /* no CUDA device / not an sm_100 device   */
+#define GG_ERR_TOO_LARGE (-7)   /* beyond gg_render_device_noalloc's fixed scratch */
 
 /* ---- metric (gr-core Metric implementations) --------------------------- */
 #define GG_METRIC_SCHWARZSCHILD 0
@@ -211,6 +212,34 @@ GG_API int gg_render_device(gg_ctx* ctx, const gg_metric_t* metric, const gg_cam
                             const gg_disk_t* disk, const gg_integrator_t* integ,
                             const gg_render_opts_t* opts, uint32_t width, uint32_t height,
                             uint8_t* rgb_dev, const gg_ray_out_t* rays_dev, void* stream);
+
+/* For callers that must not let a library allocate device memory (their
+ * own arena or pool owns every byte, or allocation after start-up is
+ * forbidden, or a cudaMalloc's device-wide synchronisation is unacceptable).
+ * No counterpart in the reference, which has no device code.
+ *
+ * Same render as gg_render_device, but without a context and without any
+ * allocation: it calls no cudaMalloc / cudaFree and no allocating library
+ * routine.  Its scratch (work-queue counters and, when samples_per_axis > 1
+ * or jitter_spp > 1, one linear colour per sample) is a 16 MiB array that
+ * every GPU which loads this library holds until the process exits.
+ *   - Works on the current device; outputs are device pointers; enqueued on
+ *     `stream` (NULL = CUDA's default stream) without synchronising.
+ *   - Supersampled images are limited to 699,040 samples
+ *     (width * height * spp); larger ones return GG_ERR_TOO_LARGE.
+ *     Single-sample images have no size limit here.
+ *   - The first call on a device looks up the array's device address (once
+ *     per device); make that first call before any stream capture.
+ *   - Every call on a device shares the one array: calls whose work overlaps
+ *     on the GPU (different streams, not ordered) race and corrupt each
+ *     other's results.  Order them, for example on one stream.
+ *   - The attempt budget and the mixed precision form are not offered here
+ *     (GG_ERR_UNSUPPORTED); no statistics are returned. */
+GG_API int gg_render_device_noalloc(const gg_metric_t* metric, const gg_camera_t* camera,
+                                    const gg_disk_t* disk, const gg_integrator_t* integ,
+                                    const gg_render_opts_t* opts, uint32_t width,
+                                    uint32_t height, uint8_t* rgb_dev,
+                                    const gg_ray_out_t* rays_dev, void* stream);
 
 /* ---- measurement ------------------------------------------------------- */
 /* FMA throughput of the context's device in FLOP/s (an FMA counts 2), best
