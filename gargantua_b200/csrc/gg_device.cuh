@@ -323,32 +323,26 @@ struct DP {
 // Stage position pos + (h a_i) vel (the reference moves stage positions
 // along the step's initial velocity, geodesic.rs:248-284); returns false
 // when the reference's is_valid_position would reject it.
+// Uncontracted like the reference's `pos + h*a*vel`, so the last stage's
+// position (ha = h) equals the accepted position bit for bit, which is what
+// lets k7 serve as the next step's k1.
 GG_DEV bool stage_pos(const Ray& R, double ha, double& r, double& th) {
-  const double t = R.x[0] + ha * R.v[0];
-  r = R.x[1] + ha * R.v[1];
-  th = R.x[2] + ha * R.v[2];
-  const double ph = R.x[3] + ha * R.v[3];
+  const double t = add_rn(R.x[0], mul_rn(ha, R.v[0]));
+  r = add_rn(R.x[1], mul_rn(ha, R.v[1]));
+  th = add_rn(R.x[2], mul_rn(ha, R.v[2]));
+  const double ph = add_rn(R.x[3], mul_rn(ha, R.v[3]));
   return finite4(t, r, th, ph) && r > 0.0;
 }
 
-// Where the stage derivatives k1..k6 live between the stages of an attempt:
-// registers, or (GG_K_SHARED) this thread's column of a block-shared array,
-// [stage][component][thread] so a warp's accesses are conflict-free.  The
-// shared form frees 48 registers of the stepping loop for occupancy.
-#ifndef GG_K_SHARED
-#define GG_K_SHARED 1
-#endif
-#if GG_K_SHARED
+// Where the stage derivatives k1..k6 live between the stages of an attempt
+// (and k1 between attempts): this thread's column of a block-shared array,
+// [stage][component][thread] so a warp's accesses are conflict-free.  Kept
+// out of registers, they free 48 registers of the stepping loop for
+// occupancy.
 struct KStore {
   double (*s)[4][kTraceBlock];
   GG_DEV double& operator()(int stage, int i) const { return s[stage][i][threadIdx.x]; }
 };
-#else
-struct KStore {
-  double k[6][4];
-  GG_DEV double& operator()(int stage, int i) { return k[stage][i]; }
-};
-#endif
 
 // v + h (c1 k1 + c3 k3 + c4 k4 + c5 k5 + c6 k6), left to right, uncontracted
 // (geodesic.rs:294-295).
@@ -375,18 +369,22 @@ GG_DEV double combine4(double v, double h, double k1, double k3, double k4, doub
 // One call of RK45Integrator::step (geodesic.rs:185-328) in FP64.
 // Returns the StepResult; `accepted` and `h_used` describe an advance.
 template <int METRIC>
-GG_DEV int attempt_fp64(const DevParams& P, Ray& R, bool& accepted, double& h_used) {
+//
+// `k1_valid` says K(0, .) already holds a(x, v) for the current state: the
+// reference's k7 is evaluated at (pos + h vel, new_vel), exactly the state an
+// accepted step moves to, so it is the next attempt's k1 (first same as
+// last) unless normalisation reflected theta at a pole; a rejected attempt
+// leaves the state, and so k1, unchanged.  The reference recomputes k1; the
+// values are identical, one right-hand side per attempt cheaper.
+GG_DEV int attempt_fp64(const DevParams& P, Ray& R, bool& k1_valid, bool& accepted,
+                        double& h_used) {
   accepted = false;
   if (R.x[1] > P.max_radius) return kEscaped;
   if (P.has_horizon && (R.x[1] < P.rh_plus_buffer || R.x[1] < P.rh)) return kHorizon;
 
   const double h = R.h;
-#if GG_K_SHARED
   __shared__ double k_smem[6][4][kTraceBlock];
   KStore K{k_smem};
-#else
-  KStore K;
-#endif
   double k7[4], nv[4];
   double r = R.x[1], th = R.x[2];
   // The right-hand-side evaluations run as one loop so the RHS code (sincos,
@@ -395,8 +393,12 @@ GG_DEV int attempt_fp64(const DevParams& P, Ray& R, bool& accepted, double& h_us
   // inputs and the k registers are selected per stage by switch arms
   // (warp-uniform branches; all lanes of a warp run the same stage).  The
   // last pass evaluates k6 and k7, which share the position pos6.
+  // Warp-uniform first stage: a lane whose k1 is valid recomputes the same
+  // value when a refilled lane in its warp needs k1, instead of the warp
+  // running the whole attempt diverged.
+  const int s_first = __any_sync(__activemask(), !k1_valid) ? 0 : 1;
 #pragma unroll 1
-  for (int s = 0; s < 6; ++s) {
+  for (int s = s_first; s < 6; ++s) {
     double w[4];
     switch (s) {
       case 0:
@@ -504,7 +506,13 @@ GG_DEV int attempt_fp64(const DevParams& P, Ray& R, bool& accepted, double& h_us
 #pragma unroll
     for (int i = 0; i < 4; ++i) R.v[i] = nv[i];
     R.lam = add_rn(R.lam, h);
+    const bool reflected = R.x[2] < 0.0 || R.x[2] > kPi;
     normalize_coords(R.x);
+    if (!reflected) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i) K(0, i) = k7[i];
+    }
+    k1_valid = !reflected;
     accepted = true;
     h_used = h;
     if (err > 0.0) {

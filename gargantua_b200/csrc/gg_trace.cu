@@ -150,6 +150,7 @@ __global__ void __launch_bounds__(kTraceBlock,
   uint32_t n_att = 0, n_acc = 0;
   double inten = 0.0, trans = 1.0;  // volumetric disk accumulators
   bool crossed = false;
+  bool k1_valid = false;  // K(0, .) holds a(x, v) of the current state
 
   uint64_t wbase = 0;
   uint32_t wcount = 0;
@@ -198,6 +199,7 @@ __global__ void __launch_bounds__(kTraceBlock,
         inten = 0.0;
         trans = 1.0;
         crossed = false;
+        k1_valid = false;
       }
       wbase += take;
       wcount -= take;
@@ -218,7 +220,7 @@ __global__ void __launch_bounds__(kTraceBlock,
       const double lam_b = R.lam;
       bool acc;
       double h_used = 0.0;
-      const int res = attempt_fp64<METRIC>(P, R, acc, h_used);
+      const int res = attempt_fp64<METRIC>(P, R, k1_valid, acc, h_used);
       n_att += 1;
       if (acc) n_acc += 1;
       int done_cls = -1;
