@@ -33,6 +33,8 @@ GG_DISK_VOLUMETRIC = 1
 GG_DISK_THIN = 2
 GG_PREC_FP64 = 0
 GG_PREC_MIXED = 1
+GG_STEPPER_REFERENCE = 0
+GG_STEPPER_DP45 = 1
 GG_SKY_PROCEDURAL = 0
 GG_SKY_CHECKER = 1
 
@@ -65,7 +67,7 @@ class gg_integrator_t(C.Structure):
                 ("max_step", C.c_double), ("tolerance", C.c_double),
                 ("max_radius", C.c_double), ("horizon_buffer", C.c_double),
                 ("rtol", C.c_double), ("atol", C.c_double), ("max_steps", C.c_uint32),
-                ("precision", C.c_int32)]
+                ("precision", C.c_int32), ("stepper", C.c_int32), ("reserved", C.c_int32)]
 
 
 class gg_render_opts_t(C.Structure):

@@ -151,6 +151,8 @@ int validate(const gg_metric_t* metric, const gg_camera_t* camera, const gg_disk
   if (integ->max_steps < 1) return GG_ERR_INVALID_ARG;
   if (integ->precision != GG_PREC_FP64 && integ->precision != GG_PREC_MIXED)
     return GG_ERR_INVALID_ARG;
+  if (integ->stepper != GG_STEPPER_REFERENCE && integ->stepper != GG_STEPPER_DP45)
+    return GG_ERR_INVALID_ARG;
   if (opts->sky != GG_SKY_PROCEDURAL && opts->sky != GG_SKY_CHECKER) return GG_ERR_INVALID_ARG;
   if (opts->sky == GG_SKY_CHECKER && (opts->sky_rows < 1 || opts->sky_cols < 1))
     return GG_ERR_INVALID_ARG;
@@ -196,6 +198,7 @@ void build_params(const gg_metric_t* metric, const gg_camera_t* camera, const gg
   P.atol = integ->atol;
   P.max_steps = integ->max_steps;
   P.precision = integ->precision;
+  P.stepper = integ->stepper == GG_STEPPER_DP45 ? gg::kStepperDP45 : gg::kStepperReference;
 
   P.width = width;
   P.height = height;

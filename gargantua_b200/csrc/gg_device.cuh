@@ -340,7 +340,7 @@ GG_DEV bool stage_pos(const Ray& R, double ha, double& r, double& th) {
 // out of registers, they free 48 registers of the stepping loop for
 // occupancy.
 struct KStore {
-  double (*s)[4][kTraceBlock];
+  double (*s)[4][kTraceBlock];  // [7][4][kTraceBlock], declared by the kernel
   GG_DEV double& operator()(int stage, int i) const { return s[stage][i][threadIdx.x]; }
 };
 
@@ -376,15 +376,13 @@ template <int METRIC>
 // last) unless normalisation reflected theta at a pole; a rejected attempt
 // leaves the state, and so k1, unchanged.  The reference recomputes k1; the
 // values are identical, one right-hand side per attempt cheaper.
-GG_DEV int attempt_fp64(const DevParams& P, Ray& R, bool& k1_valid, bool& accepted,
-                        double& h_used) {
+GG_DEV int attempt_fp64(const DevParams& P, Ray& R, const KStore& K, bool& k1_valid,
+                        bool& accepted, double& h_used) {
   accepted = false;
   if (R.x[1] > P.max_radius) return kEscaped;
   if (P.has_horizon && (R.x[1] < P.rh_plus_buffer || R.x[1] < P.rh)) return kHorizon;
 
   const double h = R.h;
-  __shared__ double k_smem[6][4][kTraceBlock];
-  KStore K{k_smem};
   double k7[4], nv[4];
   double r = R.x[1], th = R.x[2];
   // The right-hand-side evaluations run as one loop so the RHS code (sincos,
@@ -525,6 +523,230 @@ GG_DEV int attempt_fp64(const DevParams& P, Ray& R, bool& k1_valid, bool& accept
     R.h = fmax(h * 0.9 * sqrt(sqrt(tol / err)), P.min_step);
   }
   return kContinue;
+}
+
+// ---------------------------------------------------------------------------
+// Full Dormand-Prince RK5(4) on y = (x, v) (GG_STEPPER_DP45).
+//
+// y'' = a(y, y') is second order, so every stage position and the error of
+// the positions can be written with the stage accelerations alone (Nystrom
+// form): x_s = x + h a_s v + h^2 sum_l Abar[s][l] k_l with Abar = B B,
+// x_new = x + h v + h^2 sum_l Cbar_l k_l, and x_new - x_err =
+// h^2 sum_l Ebar_l k_l (the plain weights c and d both sum to 1).  No stage
+// velocity needs storing; only the k's, which live in shared memory and are
+// indexed by the stage loop directly.
+// ---------------------------------------------------------------------------
+struct DPTable {
+  double B[7][7];     // stage velocity: v_s = v + h sum_l B[s][l] k_l (row 6 = c)
+  double Abar[7][7];  // stage position, coefficient of h^2 k_l
+  double A[7];        // stage node a_s (row sums of B)
+  double E[7];        // c - d, velocity error weights
+  double Ebar[7];     // position error weights of h^2 k_l
+};
+
+constexpr DPTable make_dp_table() {
+  DPTable t{};
+  const double b[7][7] = {
+      {0, 0, 0, 0, 0, 0, 0},
+      {1.0 / 5.0, 0, 0, 0, 0, 0, 0},
+      {3.0 / 40.0, 9.0 / 40.0, 0, 0, 0, 0, 0},
+      {44.0 / 45.0, -56.0 / 15.0, 32.0 / 9.0, 0, 0, 0, 0},
+      {19372.0 / 6561.0, -25360.0 / 2187.0, 64448.0 / 6561.0, -212.0 / 729.0, 0, 0, 0},
+      {9017.0 / 3168.0, -355.0 / 33.0, 46732.0 / 5247.0, 49.0 / 176.0, -5103.0 / 18656.0, 0, 0},
+      {35.0 / 384.0, 0.0, 500.0 / 1113.0, 125.0 / 192.0, -2187.0 / 6784.0, 11.0 / 84.0, 0}};
+  const double d[7] = {5179.0 / 57600.0, 0.0, 7571.0 / 16695.0, 393.0 / 640.0,
+                       -92097.0 / 339200.0, 187.0 / 2100.0, 1.0 / 40.0};
+  for (int s = 0; s < 7; ++s) {
+    double a = 0.0;
+    for (int l = 0; l < 7; ++l) {
+      t.B[s][l] = b[s][l];
+      a += b[s][l];
+      double ab = 0.0;
+      for (int j = l + 1; j < s; ++j) ab += b[s][j] * b[j][l];
+      t.Abar[s][l] = ab;
+    }
+    t.A[s] = a;
+  }
+  for (int l = 0; l < 7; ++l) {
+    const double c_l = l < 6 ? b[6][l] : 0.0;
+    t.E[l] = c_l - d[l];
+    // x_err uses d_j times stage velocities j = 1..7, the 7th being v_new
+    // (row 6 of b is c, and c_7 = b[6][6] = 0)
+    double eb = 0.0;
+    for (int j = l + 1; j < 7; ++j) eb += (b[6][j] - d[j]) * b[j][l];
+    t.Ebar[l] = eb;
+  }
+  return t;
+}
+
+__constant__ DPTable kDP = make_dp_table();
+
+// State at the end of an accepted full Dormand-Prince step, for the
+// crossing interpolant (a at both ends sits in K(0, .) and K(6, .)).
+struct StepEnd {
+  double xraw[4];  // new position before angle normalisation
+};
+
+// One full Dormand-Prince attempt in FP64.  Same contract as attempt_fp64;
+// with k1_valid the previous step's last stage (K(6, .), evaluated at the
+// accepted state) is copied to K(0, .) first.
+template <int METRIC>
+GG_DEV int attempt_dp45_fp64(const DevParams& P, Ray& R, const KStore& K, bool& k1_valid,
+                             bool& k7_pending, bool& accepted, double& h_used, StepEnd& end) {
+  accepted = false;
+  if (R.x[1] > P.max_radius) return kEscaped;
+  if (P.has_horizon && (R.x[1] < P.rh_plus_buffer || R.x[1] < P.rh)) return kHorizon;
+  if (k7_pending) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) K(0, i) = K(6, i);
+    k7_pending = false;
+  }
+  const double h = R.h, hh = h * h;
+  double xn[4], vn[4];
+  const int s_first = __any_sync(__activemask(), !k1_valid) ? 0 : 1;
+#pragma unroll 1
+  for (int s = s_first; s < 7; ++s) {
+    double px[4], pw[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      px[i] = R.x[i];
+      pw[i] = R.v[i];
+    }
+    if (s > 0) {
+      const double ha = h * kDP.A[s];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) px[i] = fma(ha, R.v[i], px[i]);
+#pragma unroll 1
+      for (int l = 0; l < s; ++l) {
+        const double cb = hh * kDP.Abar[s][l], cv = h * kDP.B[s][l];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const double kl = K(l, i);
+          px[i] = fma(cb, kl, px[i]);
+          pw[i] = fma(cv, kl, pw[i]);
+        }
+      }
+      if (!(finite4(px[0], px[1], px[2], px[3]) && px[1] > 0.0)) {
+        R.h = h * 0.5;
+        return kContinue;
+      }
+    }
+    Geometry<METRIC> G;
+    G.at(P, px[1], px[2]);
+    double a[4];
+    G.accel(pw, a);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) K(s, i) = a[i];
+    if (s == 6) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        xn[i] = px[i];
+        vn[i] = pw[i];
+      }
+    }
+  }
+  // embedded error of positions (h^2 sum Ebar k) and velocities (h sum E k)
+  double ex[4] = {0.0, 0.0, 0.0, 0.0}, ev[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 1
+  for (int l = 0; l < 7; ++l) {
+    const double eb = kDP.Ebar[l], e = kDP.E[l];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const double kl = K(l, i);
+      ex[i] = fma(eb, kl, ex[i]);
+      ev[i] = fma(e, kl, ev[i]);
+    }
+  }
+  double err, tol;
+  double s2 = 0.0;
+  if (P.rtol > 0.0) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const double qx = hh * ex[i] / (P.atol + P.rtol * fmax(fabs(R.x[i]), fabs(xn[i])));
+      const double qv = h * ev[i] / (P.atol + P.rtol * fmax(fabs(R.v[i]), fabs(vn[i])));
+      s2 = s2 + qx * qx + qv * qv;
+    }
+    err = sqrt(s2 * 0.125);
+    tol = 1.0;
+  } else {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) s2 = s2 + (hh * ex[i]) * (hh * ex[i]) + (h * ev[i]) * (h * ev[i]);
+    err = sqrt(s2);
+    tol = P.tolerance;
+  }
+  if (err < tol || h <= P.min_step) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      end.xraw[i] = xn[i];
+      R.x[i] = xn[i];
+      R.v[i] = vn[i];
+    }
+    R.lam = R.lam + h;
+    const bool reflected = R.x[2] < 0.0 || R.x[2] > kPi;
+    normalize_coords(R.x);
+    // K(6, .) = a(x_new, v_new): the next k1 unless theta was reflected;
+    // copied at the next attempt so the caller can still read this step's k1
+    k1_valid = !reflected;
+    k7_pending = !reflected;
+    accepted = true;
+    h_used = h;
+    if (err > 0.0) {
+      double hn = h * 0.9 * fifth_root(tol / err);
+      hn = hn < P.min_step ? P.min_step : (hn > P.max_step ? P.max_step : hn);
+      R.h = hn;
+    }
+  } else {
+    R.h = fmax(h * 0.9 * sqrt(sqrt(tol / err)), P.min_step);
+  }
+  return kContinue;
+}
+
+// Cubic Hermite interpolant of an accepted full Dormand-Prince step at
+// fraction s: positions from (x, v) at both ends, velocities from (v, a).
+GG_DEV void hermite_point(const double xb[4], const double vb[4], const double kb[4],
+                          const double xa[4], const double va[4], const double ka[4], double h,
+                          double s, double out[8]) {
+  const double s2 = s * s, s3 = s2 * s;
+  const double h00 = 2.0 * s3 - 3.0 * s2 + 1.0, h10 = s3 - 2.0 * s2 + s;
+  const double h01 = -2.0 * s3 + 3.0 * s2, h11 = s3 - s2;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    out[i] = h00 * xb[i] + h10 * h * vb[i] + h01 * xa[i] + h11 * h * va[i];
+    out[4 + i] = h00 * vb[i] + h10 * h * kb[i] + h01 * va[i] + h11 * h * ka[i];
+  }
+}
+
+// Fraction s where component c of the Hermite position meets `target`
+// (bracketed by the step's ends): safeguarded Newton, at most 30 steps.
+GG_DEV double hermite_root(const double xb[4], const double vb[4], const double xa[4],
+                           const double va[4], double h, int c, double target) {
+  const double p0 = xb[c], m0 = h * vb[c], p1 = xa[c], m1 = h * va[c];
+  auto f = [&](double s, double& df) {
+    const double s2 = s * s, s3 = s2 * s;
+    df = (6.0 * s2 - 6.0 * s) * p0 + (3.0 * s2 - 4.0 * s + 1.0) * m0 + (-6.0 * s2 + 6.0 * s) * p1 +
+         (3.0 * s2 - 2.0 * s) * m1;
+    return (2.0 * s3 - 3.0 * s2 + 1.0) * p0 + (s3 - 2.0 * s2 + s) * m0 +
+           (-2.0 * s3 + 3.0 * s2) * p1 + (s3 - s2) * m1 - target;
+  };
+  double lo = 0.0, hi = 1.0, d0, d1;
+  const double flo = f(0.0, d0);
+  const double fhi = f(1.0, d1);
+  double s = flo / (flo - fhi);
+  if (!(s >= 0.0 && s <= 1.0)) s = 0.5;
+  for (int it = 0; it < 30; ++it) {
+    double d;
+    const double fs = f(s, d);
+    if (fs == 0.0) break;
+    if ((fs < 0.0) == (flo < 0.0)) lo = s; else hi = s;
+    double sn = d != 0.0 ? s - fs / d : 0.5 * (lo + hi);
+    if (!(sn > lo && sn < hi)) sn = 0.5 * (lo + hi);
+    if (fabs(sn - s) <= 1e-15) {
+      s = sn;
+      break;
+    }
+    s = sn;
+  }
+  return s;
 }
 
 // ---------------------------------------------------------------------------

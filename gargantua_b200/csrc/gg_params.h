@@ -16,6 +16,7 @@ enum : int { kMetricSchwarzschild = 0, kMetricKerr = 1 };
 enum : int { kDiskNone = 0, kDiskVolumetric = 1, kDiskThin = 2 };
 enum : int { kSkyProcedural = 0, kSkyChecker = 1 };
 enum : int { kClsHorizon = 0, kClsEscaped = 1, kClsDisk = 2, kClsMaxSteps = 3, kClsBudget = 4 };
+enum : int { kStepperReference = 0, kStepperDP45 = 1 };
 
 struct DevParams {
   // metric
@@ -29,6 +30,8 @@ struct DevParams {
   double rtol, atol;
   uint32_t max_steps;
   int precision;
+  int stepper;
+  int pad_stepper;
   // sampling
   uint32_t width, height, spa, spp, jitter_spp, sub_w, sub_h;
   uint32_t pad0;

@@ -126,13 +126,15 @@ GG_DEV void store_cross(const DevParams& P, const DevOutputs& O, uint64_t idx,
   for (int i = 0; i < 8; ++i) O.cross[i * P.n_rays + idx] = c[i];
 }
 
-template <int METRIC, int DISK>
+template <int METRIC, int DISK, int STEPPER>
 __global__ void __launch_bounds__(kTraceBlock,
                                   METRIC == kMetricKerr ? kTraceMinBlocksKerr : kTraceMinBlocksSchw)
     trace_fp64_kernel(const __grid_constant__ DevParams P, const __grid_constant__ DevOutputs O,
                       DevControl* ctl) {
   const unsigned lane = threadIdx.x & 31u;
   __shared__ BlockStats bs;
+  __shared__ double k_smem[7][4][kTraceBlock];  // stage derivatives, see KStore
+  const KStore K{k_smem};
   if (threadIdx.x < sizeof(BlockStats) / 8)
     reinterpret_cast<unsigned long long*>(&bs)[threadIdx.x] = 0ull;
   __syncthreads();
@@ -150,7 +152,8 @@ __global__ void __launch_bounds__(kTraceBlock,
   uint32_t n_att = 0, n_acc = 0;
   double inten = 0.0, trans = 1.0;  // volumetric disk accumulators
   bool crossed = false;
-  bool k1_valid = false;  // K(0, .) holds a(x, v) of the current state
+  bool k1_valid = false;    // K(0, .) holds a(x, v) of the current state
+  bool k7_pending = false;  // full DP: K(6, .) is the next k1, copy pending
 
   uint64_t wbase = 0;
   uint32_t wcount = 0;
@@ -200,6 +203,7 @@ __global__ void __launch_bounds__(kTraceBlock,
         trans = 1.0;
         crossed = false;
         k1_valid = false;
+        k7_pending = false;
       }
       wbase += take;
       wcount -= take;
@@ -220,18 +224,46 @@ __global__ void __launch_bounds__(kTraceBlock,
       const double lam_b = R.lam;
       bool acc;
       double h_used = 0.0;
-      const int res = attempt_fp64<METRIC>(P, R, k1_valid, acc, h_used);
+      StepEnd end;
+      int res;
+      if (STEPPER == kStepperDP45)
+        res = attempt_dp45_fp64<METRIC>(P, R, K, k1_valid, k7_pending, acc, h_used, end);
+      else
+        res = attempt_fp64<METRIC>(P, R, K, k1_valid, acc, h_used);
       n_att += 1;
       if (acc) n_acc += 1;
       int done_cls = -1;
       double out_int = 0.0, out_temp = 0.0;
 
       if (acc) {
+        // The step's path: the reference's Euler segment (exactly linear in
+        // the step fraction), or the full Dormand-Prince step's cubic Hermite.
+        double raw[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          raw[i] = STEPPER == kStepperDP45 ? end.xraw[i] : xb[i] + h_used * vb[i];
+        auto point = [&](double s, double c[8]) {
+          if (STEPPER == kStepperDP45) {
+            double ka[4], kb[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+              kb[i] = K(0, i);
+              ka[i] = K(6, i);
+            }
+            hermite_point(xb, vb, kb, raw, R.v, ka, h_used, s, c);
+            normalize_coords(c);
+          } else {
+            segment_point(xb, vb, h_used, R.v, s, c);
+          }
+        };
+        auto root = [&](int comp, double target, double linear_s) {
+          return STEPPER == kStepperDP45 ? hermite_root(xb, vb, raw, R.v, h_used, comp, target)
+                                         : linear_s;
+        };
         // escape-sphere crossing on this step
-        const double raw_r = xb[1] + h_used * vb[1];
-        if (O.cross && xb[1] <= P.max_radius && raw_r > P.max_radius) {
+        if (O.cross && xb[1] <= P.max_radius && raw[1] > P.max_radius) {
           double c[8];
-          segment_point(xb, vb, h_used, R.v, (P.max_radius - xb[1]) / (raw_r - xb[1]), c);
+          point(root(1, P.max_radius, (P.max_radius - xb[1]) / (raw[1] - xb[1])), c);
           store_cross(P, O, idx, c);
           crossed = true;
         }
@@ -239,11 +271,12 @@ __global__ void __launch_bounds__(kTraceBlock,
           const double d_b = xb[2] - kHalfPi;
           const double d_a = R.x[2] - kHalfPi;
           if ((d_b < 0.0 && d_a >= 0.0) || (d_b > 0.0 && d_a <= 0.0)) {
-            const double s = d_b / (d_b - d_a);
-            const double r_c = xb[1] + s * (raw_r - xb[1]);
+            const double s = root(2, kHalfPi, d_b / (d_b - d_a));
+            double c[8];
+            point(s, c);
+            const double r_c =
+                STEPPER == kStepperDP45 ? c[1] : xb[1] + s * (raw[1] - xb[1]);
             if (r_c >= P.r_inner && r_c <= P.r_outer) {
-              double c[8];
-              segment_point(xb, vb, h_used, R.v, s, c);
               c[1] = r_c;
               c[2] = kHalfPi;
               const double g = redshift_factor<METRIC>(P, r_c, kHalfPi, c + 4);
@@ -374,20 +407,26 @@ __global__ void reduce_samples_kernel(const __grid_constant__ DevParams P, const
   }
 }
 
-template <int METRIC, int DISK>
+template <int METRIC, int DISK, int STEPPER>
 const void* trace_fn() {
-  return reinterpret_cast<const void*>(&trace_fp64_kernel<METRIC, DISK>);
+  return reinterpret_cast<const void*>(&trace_fp64_kernel<METRIC, DISK, STEPPER>);
+}
+
+template <int STEPPER>
+const void* select_metric_disk(const DevParams& P) {
+  if (P.metric == kMetricKerr) {
+    if (P.disk == kDiskThin) return trace_fn<kMetricKerr, kDiskThin, STEPPER>();
+    if (P.disk == kDiskVolumetric) return trace_fn<kMetricKerr, kDiskVolumetric, STEPPER>();
+    return trace_fn<kMetricKerr, kDiskNone, STEPPER>();
+  }
+  if (P.disk == kDiskThin) return trace_fn<kMetricSchwarzschild, kDiskThin, STEPPER>();
+  if (P.disk == kDiskVolumetric) return trace_fn<kMetricSchwarzschild, kDiskVolumetric, STEPPER>();
+  return trace_fn<kMetricSchwarzschild, kDiskNone, STEPPER>();
 }
 
 const void* select_trace(const DevParams& P) {
-  if (P.metric == kMetricKerr) {
-    if (P.disk == kDiskThin) return trace_fn<kMetricKerr, kDiskThin>();
-    if (P.disk == kDiskVolumetric) return trace_fn<kMetricKerr, kDiskVolumetric>();
-    return trace_fn<kMetricKerr, kDiskNone>();
-  }
-  if (P.disk == kDiskThin) return trace_fn<kMetricSchwarzschild, kDiskThin>();
-  if (P.disk == kDiskVolumetric) return trace_fn<kMetricSchwarzschild, kDiskVolumetric>();
-  return trace_fn<kMetricSchwarzschild, kDiskNone>();
+  return P.stepper == kStepperDP45 ? select_metric_disk<kStepperDP45>(P)
+                                   : select_metric_disk<kStepperReference>(P);
 }
 
 }  // namespace

@@ -97,6 +97,9 @@ class RK45Integrator:
     horizon_buffer: float = 0.01
     rtol: float = 0.0
     atol: float = 0.0
+    # extension: abi.GG_STEPPER_DP45 runs the full Dormand-Prince method on
+    # (x, v) instead of the reference's step (see include/gargantua_gpu.h)
+    stepper: int = abi.GG_STEPPER_REFERENCE
 
     def to_c(self, max_steps: int, precision: int = abi.GG_PREC_FP64) -> abi.gg_integrator_t:
         k = abi.gg_integrator_t()
@@ -110,6 +113,7 @@ class RK45Integrator:
         k.atol = self.atol
         k.max_steps = int(max_steps)
         k.precision = int(precision)
+        k.stepper = int(self.stepper)
         return k
 
 

@@ -3,7 +3,9 @@
 Each function returns a ``Scene`` for one workload by what it is and its
 sizes.  The integrator of the disk workloads is the reference's RK45 with
 its step bounds and a mixed rtol = 1e-8 / atol = 1e-10 error norm, 10,000
-step() calls per ray, escape at r = 200 (renderer.rs:264).
+step() calls per ray, escape at r = 200 (renderer.rs:264); `stepper`
+selects the reference's step or the full Dormand-Prince method
+(abi.GG_STEPPER_DP45), which the precision comparison needs.
 """
 from __future__ import annotations
 
@@ -15,8 +17,8 @@ from .curved import (AccretionDisk, Camera, CheckerSky, ProceduralSky, RenderOpt
 from .gr_core import Kerr, RK45Integrator, Schwarzschild
 
 
-def disk_integrator() -> RK45Integrator:
-    return RK45Integrator(max_radius=200.0, rtol=1e-8, atol=1e-10)
+def disk_integrator(stepper: int = abi.GG_STEPPER_REFERENCE) -> RK45Integrator:
+    return RK45Integrator(max_radius=200.0, rtol=1e-8, atol=1e-10, stepper=stepper)
 
 
 def reference_cli(width: int = 800, height: int = 600, metric: str = "schwarzschild",
@@ -31,32 +33,35 @@ def reference_cli(width: int = 800, height: int = 600, metric: str = "schwarzsch
                  RenderOptions(samples_per_axis=samples, sky=ProceduralSky()))
 
 
-def schwarzschild_thin_256(precision: int = abi.GG_PREC_FP64) -> Scene:
+def schwarzschild_thin_256(precision: int = abi.GG_PREC_FP64,
+                           stepper: int = abi.GG_STEPPER_REFERENCE) -> Scene:
     """Schwarzschild M=1, 256x256, 1 spp, camera r=30 at 80 deg inclination, 60 deg
     FOV, thin disk 6-20 M (q=3), 18x36 checkerboard sky seed 0, all f64."""
     return Scene(Schwarzschild(1.0),
                  Camera.inclined(30.0, math.radians(80.0), math.radians(60.0), 1.0), 256, 256,
                  ThinDisk(6.0, 20.0, 3.0),
                  RenderOptions(sky=CheckerSky(18, 36, 0), max_steps=10000,
-                               integrator=disk_integrator(), precision=precision))
+                               integrator=disk_integrator(stepper), precision=precision))
 
 
-def kerr_thin_1080p(spin: float = 0.9, precision: int = abi.GG_PREC_FP64) -> Scene:
+def kerr_thin_1080p(spin: float = 0.9, precision: int = abi.GG_PREC_FP64,
+                    stepper: int = abi.GG_STEPPER_REFERENCE) -> Scene:
     """Kerr a=0.9, 1920x1080, camera r=50 at 75 deg, disk r_ISCO-30 M (q=3),
     the same checkerboard sky and integrator as the 256x256 Schwarzschild scene."""
     k = Kerr(1.0, spin)
     return Scene(k, Camera.inclined(50.0, math.radians(75.0), math.radians(60.0), 1920 / 1080),
                  1920, 1080, ThinDisk(k.isco(), 30.0, 3.0),
                  RenderOptions(sky=CheckerSky(18, 36, 0), max_steps=10000,
-                               integrator=disk_integrator(), precision=precision))
+                               integrator=disk_integrator(stepper), precision=precision))
 
 
-def kerr_stress_4k(precision: int = abi.GG_PREC_FP64, side: int = 4096, spp: int = 16) -> Scene:
+def kerr_stress_4k(precision: int = abi.GG_PREC_FP64, side: int = 4096, spp: int = 16,
+                   stepper: int = abi.GG_STEPPER_REFERENCE) -> Scene:
     """Near-extremal Kerr a=0.998, 4096x4096, 16 seeded jittered samples per
     pixel, camera r=15 at 85 deg, disk r_ISCO-25 M, 50,000 step() calls."""
     k = Kerr(1.0, 0.998)
     return Scene(k, Camera.inclined(15.0, math.radians(85.0), math.radians(60.0), 1.0), side,
                  side, ThinDisk(k.isco(), 25.0, 3.0),
                  RenderOptions(sky=CheckerSky(18, 36, 0), jitter_spp=spp, seed=1,
-                               max_steps=50000, integrator=disk_integrator(),
+                               max_steps=50000, integrator=disk_integrator(stepper),
                                precision=precision))

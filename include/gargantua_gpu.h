@@ -90,6 +90,14 @@ typedef struct gg_disk_t {
 #define GG_PREC_FP64 0  /* plain FP64, the drop-in                           */
 #define GG_PREC_MIXED 1 /* FP32 stages + compensated state, FP64 controller  */
 
+/* The reference's RK45Integrator::step (geodesic.rs:185-328) moves the
+ * position by h * vel (first order) and controls the velocity error only.
+ * GG_STEPPER_DP45 is the full Dormand-Prince RK5(4) on (x, v): positions
+ * from the stage velocities, error control over all eight components, the
+ * reference's termination tests and step-size law, cubic Hermite crossings. */
+#define GG_STEPPER_REFERENCE 0
+#define GG_STEPPER_DP45 1
+
 typedef struct gg_integrator_t {
   double initial_step;
   double min_step;
@@ -101,6 +109,8 @@ typedef struct gg_integrator_t {
   double atol;
   uint32_t max_steps;    /* step() calls per ray before MaxSteps             */
   int32_t precision;     /* GG_PREC_*                                        */
+  int32_t stepper;       /* GG_STEPPER_*                                     */
+  int32_t reserved;
 } gg_integrator_t;
 
 /* ---- render options (raytracer::curved::RenderOptions) ----------------- */

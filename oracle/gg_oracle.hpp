@@ -549,11 +549,18 @@ struct RK45 {
   // by an RMS norm of the same difference scaled per component by
   // atol + rtol * max(|vel_i|, |new_vel_i|), compared against 1.
   double rtol = 0.0, atol = 0.0;
+  // EXTENSION: stepper 1 is the full Dormand-Prince method on the 8-component
+  // state (see step_dp45); 0 is the reference's step.
+  int stepper = 0;
 
   // One attempt.  `accepted` (optional) reports whether the state advanced.
+  // k_ends (optional, 12 doubles) receives a(x, v) at the start and the end
+  // of an accepted full Dormand-Prince step and its un-normalised end
+  // position, for the crossing interpolant.
   template <class M, class T>
   StepResult step(const M& metric, State<T>& st, T& h, bool* accepted = nullptr,
-                  T* h_used = nullptr) const {
+                  T* h_used = nullptr, T* k_ends = nullptr) const {
+    if (stepper == 1) return step_dp45(metric, st, h, accepted, h_used, k_ends);
     using std::fabs;
     using std::pow;
     using std::sqrt;
@@ -631,7 +638,158 @@ struct RK45 {
     }
     return kContinue;
   }
+
+  // EXTENSION: the full Dormand-Prince RK5(4) method on y = (x, v), y' =
+  // (v, a(x, v)): stage positions use the stage velocities (the reference
+  // moves positions along the step's initial velocity only, geodesic.rs:248,
+  // 312), the 5th-order solution advances x and v, and the embedded error
+  // h * sum_j (c_j - d_j) F_j covers all eight components.  Termination
+  // tests, invalid-stage halving, the acceptance test and the step-size law
+  // are the reference's (geodesic.rs:195-207, 250-290, 310-325); with rtol > 0
+  // the norm is the RMS of the components scaled by atol + rtol*max(|y|,|y'|).
+  template <class M, class T>
+  StepResult step_dp45(const M& metric, State<T>& st, T& h, bool* accepted, T* h_used,
+                       T* k_ends) const {
+    using std::fabs;
+    using std::pow;
+    using std::sqrt;
+    if (accepted) *accepted = false;
+    const V4<T> x = st.position, v = st.velocity;
+    if (x[1] > T(max_radius)) return kEscaped;
+    double rh;
+    if (metric.event_horizon(&rh) && (x[1] < T(rh + horizon_buffer) || x[1] < T(rh)))
+      return kHorizon;
+
+    const double B[7][6] = {
+        {0, 0, 0, 0, 0, 0},
+        {1.0 / 5.0, 0, 0, 0, 0, 0},
+        {3.0 / 40.0, 9.0 / 40.0, 0, 0, 0, 0},
+        {44.0 / 45.0, -56.0 / 15.0, 32.0 / 9.0, 0, 0, 0},
+        {19372.0 / 6561.0, -25360.0 / 2187.0, 64448.0 / 6561.0, -212.0 / 729.0, 0, 0},
+        {9017.0 / 3168.0, -355.0 / 33.0, 46732.0 / 5247.0, 49.0 / 176.0, -5103.0 / 18656.0, 0},
+        {35.0 / 384.0, 0.0, 500.0 / 1113.0, 125.0 / 192.0, -2187.0 / 6784.0, 11.0 / 84.0}};
+    // 5th-order weights c (= the last row of B) and embedded 4th-order d
+    const double D[7] = {5179.0 / 57600.0, 0.0, 7571.0 / 16695.0, 393.0 / 640.0,
+                         -92097.0 / 339200.0, 187.0 / 2100.0, 1.0 / 40.0};
+    // dw[s] = w[s] - v, kept apart: the weights of the error estimate sum to
+    // zero, and summing e_j * w_j instead would leave a rounding floor of
+    // eps * |v| in the position error (it steers the step size when the true
+    // error is below it, e.g. on long escaping flights)
+    V4<T> w[7], dw[7], k[7], xs = x;
+    w[0] = v;
+    dw[0] = V4<T>{{T(0), T(0), T(0), T(0)}};
+    k[0] = metric.geodesic_acceleration(x, v);
+    for (int s = 1; s < 7; ++s) {
+      V4<T> sx{{T(0), T(0), T(0), T(0)}}, sv{{T(0), T(0), T(0), T(0)}};
+      for (int j = 0; j < s; ++j) {
+        sx = sx + T(B[s][j]) * w[j];
+        sv = sv + T(B[s][j]) * k[j];
+      }
+      xs = x + h * sx;
+      dw[s] = h * sv;
+      w[s] = v + dw[s];
+      if (!is_valid_position(xs)) {
+        h = h * T(0.5);
+        return kContinue;
+      }
+      k[s] = metric.geodesic_acceleration(xs, w[s]);  // s = 6: at the new state (FSAL)
+    }
+    // xs, w[6] are the 5th-order solution; errors from the weight differences
+    V4<T> ex{{T(0), T(0), T(0), T(0)}}, ev{{T(0), T(0), T(0), T(0)}};
+    for (int j = 0; j < 7; ++j) {
+      const T e = T((j < 6 ? B[6][j] : 0.0) - D[j]);
+      ex = ex + e * dw[j];
+      ev = ev + e * k[j];
+    }
+    ex = h * ex;
+    ev = h * ev;
+    const V4<T> xn = xs, vn = w[6];
+    T err, tol;
+    if (rtol > 0.0) {
+      T s2 = T(0.0);
+      for (int i = 0; i < 4; ++i) {
+        const T qx = ex[i] / (T(atol) + T(rtol) * rmax(fabs(x[i]), fabs(xn[i])));
+        const T qv = ev[i] / (T(atol) + T(rtol) * rmax(fabs(v[i]), fabs(vn[i])));
+        s2 = s2 + qx * qx + qv * qv;
+      }
+      err = sqrt(s2 * T(0.125));
+      tol = T(1.0);
+    } else {
+      err = sqrt(norm(ex) * norm(ex) + norm(ev) * norm(ev));
+      tol = T(tolerance);
+    }
+    if (err < tol || h <= T(min_step)) {
+      if (k_ends) {
+        for (int i = 0; i < 4; ++i) {
+          k_ends[i] = k[0][i];
+          k_ends[4 + i] = k[6][i];
+          k_ends[8 + i] = xn[i];
+        }
+      }
+      st.position = xn;
+      st.velocity = vn;
+      st.lambda = st.lambda + h;
+      normalize_spherical_coords(st.position);
+      if (accepted) *accepted = true;
+      if (h_used) *h_used = h;
+      if (err > T(0.0)) h = rclamp(h * T(0.9) * pow(tol / err, T(0.2)), min_step, max_step);
+    } else {
+      h = rmax(h * T(0.9) * pow(tol / err, T(0.25)), T(min_step));
+    }
+    return kContinue;
+  }
 };
+
+// EXTENSION: cubic Hermite interpolant of an accepted full Dormand-Prince
+// step at fraction s: position from (x, v) at both ends, velocity from (v, a).
+// xb/vb: start state; xa/va: end state before angle normalisation; ka/kb the
+// accelerations at start / end; out[8] = (x, v).
+inline void hermite_point(const double xb[4], const double vb[4], const double ka[4],
+                          const double xa[4], const double va[4], const double kb[4], double h,
+                          double s, double out[8]) {
+  const double s2 = s * s, s3 = s2 * s;
+  const double h00 = 2.0 * s3 - 3.0 * s2 + 1.0, h10 = s3 - 2.0 * s2 + s;
+  const double h01 = -2.0 * s3 + 3.0 * s2, h11 = s3 - s2;
+  for (int i = 0; i < 4; ++i) {
+    out[i] = h00 * xb[i] + h10 * h * vb[i] + h01 * xa[i] + h11 * h * va[i];
+    out[4 + i] = h00 * vb[i] + h10 * h * ka[i] + h01 * va[i] + h11 * h * kb[i];
+  }
+}
+
+// EXTENSION: fraction s in [0, 1] where component c of the Hermite position
+// equals `target`, given the interpolant changes sign there.  Newton steps
+// from the chord's root, kept inside a shrinking bracket (bisection when a
+// Newton step leaves it); 30 iterations bound the loop.
+inline double hermite_root(const double xb[4], const double vb[4], const double xa[4],
+                           const double va[4], double h, int c, double target) {
+  auto f = [&](double s, double* df) {
+    const double s2 = s * s, s3 = s2 * s;
+    const double p = (2.0 * s3 - 3.0 * s2 + 1.0) * xb[c] + (s3 - 2.0 * s2 + s) * h * vb[c] +
+                     (-2.0 * s3 + 3.0 * s2) * xa[c] + (s3 - s2) * h * va[c];
+    *df = (6.0 * s2 - 6.0 * s) * xb[c] + (3.0 * s2 - 4.0 * s + 1.0) * h * vb[c] +
+          (-6.0 * s2 + 6.0 * s) * xa[c] + (3.0 * s2 - 2.0 * s) * h * va[c];
+    return p - target;
+  };
+  double lo = 0.0, hi = 1.0, dlo, dhi;
+  const double flo = f(lo, &dlo);
+  const double fhi = f(hi, &dhi);
+  double s = flo / (flo - fhi);
+  if (!(s >= 0.0 && s <= 1.0)) s = 0.5;
+  for (int it = 0; it < 30; ++it) {
+    double d;
+    const double fs = f(s, &d);
+    if (fs == 0.0) break;
+    if ((fs < 0.0) == (flo < 0.0)) lo = s; else hi = s;
+    double sn = d != 0.0 ? s - fs / d : 0.5 * (lo + hi);
+    if (!(sn > lo && sn < hi)) sn = 0.5 * (lo + hi);
+    if (std::fabs(sn - s) <= 1e-15) {
+      s = sn;
+      break;
+    }
+    s = sn;
+  }
+  return s;
+}
 
 // ---------------------------------------------------------------------------
 // Camera and ray initialisation (crates/raytracer/src/curved/{camera,ray}.rs)
@@ -891,27 +1049,53 @@ Sample trace(const M& metric, const TraceSetup& S, const V4<double>& observer,
     State<double> before = st;
     bool acc = false;
     double h_used = 0.0;
-    StepResult result = S.integ.step(metric, st, h, &acc, &h_used);
+    double ends[12];  // full DP: a at both ends, raw end position
+    StepResult result = S.integ.step(metric, st, h, &acc, &h_used, ends);
     o.attempts += 1;
     if (acc) o.accepted += 1;
     if (acc) {
-      // the raw (un-normalised) end of the Euler segment, geodesic.rs:312
-      double dl = h_used;
+      const bool dp45 = S.integ.stepper == 1;
+      const double dl = h_used;
+      // the raw (un-normalised) end of the step: the reference's Euler segment
+      // (geodesic.rs:312), or the full Dormand-Prince solution
       V4<double> raw = before.position + dl * before.velocity;
-      // escape-sphere crossing on this segment (EXTENSION output)
+      if (dp45) raw = V4<double>{{ends[8], ends[9], ends[10], ends[11]}};
+      // state at fraction s of the step: exact on the Euler segment, cubic
+      // Hermite (EXTENSION) for the full Dormand-Prince step
+      auto point = [&](double s, double out[8]) {
+        if (!dp45) {
+          segment_point(before, raw, st.velocity, s, out);
+          return;
+        }
+        hermite_point(before.position.c, before.velocity.c, ends, raw.c, st.velocity.c,
+                      ends + 4, dl, s, out);
+        V4<double> p{{out[0], out[1], out[2], out[3]}};
+        normalize_spherical_coords(p);
+        for (int i = 0; i < 4; ++i) out[i] = p[i];
+      };
+      auto root = [&](int c, double target, double linear_s) {
+        return dp45 ? hermite_root(before.position.c, before.velocity.c, raw.c, st.velocity.c,
+                                   dl, c, target)
+                    : linear_s;
+      };
+      // escape-sphere crossing on this step (EXTENSION output)
       if (before.position[1] <= S.integ.max_radius && raw[1] > S.integ.max_radius) {
-        double s = (S.integ.max_radius - before.position[1]) / (raw[1] - before.position[1]);
-        segment_point(before, raw, st.velocity, s, o.cross);
+        double s = root(1, S.integ.max_radius,
+                        (S.integ.max_radius - before.position[1]) / (raw[1] - before.position[1]));
+        point(s, o.cross);
       }
       if (S.disk_kind == kDiskThin) {
         double d_b = before.position[2] - half_pi;
         double d_a = st.position[2] - half_pi;
         bool crossed = (d_b < 0.0 && d_a >= 0.0) || (d_b > 0.0 && d_a <= 0.0);
         if (crossed) {
-          double s = d_b / (d_b - d_a);
-          double r_c = before.position[1] + s * (raw[1] - before.position[1]);
+          double s = root(2, half_pi, d_b / (d_b - d_a));
+          double c[8];
+          point(s, c);
+          double r_c = dp45 ? c[1] : before.position[1] + s * (raw[1] - before.position[1]);
           if (r_c >= S.tdisk.r_inner && r_c <= S.tdisk.r_outer) {
-            segment_point(before, raw, st.velocity, s, o.cross);
+            for (int i = 0; i < 8; ++i) o.cross[i] = c[i];
+            o.cross[1] = r_c;
             o.cross[2] = half_pi;
             V4<double> pc{{o.cross[0], r_c, half_pi, o.cross[3]}};
             V4<double> vc{{o.cross[4], o.cross[5], o.cross[6], o.cross[7]}};

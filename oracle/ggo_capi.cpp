@@ -41,6 +41,7 @@ RK45 make_rk45(const gg_integrator_t* in) {
   k.horizon_buffer = in->horizon_buffer;
   k.rtol = in->rtol;
   k.atol = in->atol;
+  k.stepper = in->stepper;
   return k;
 }
 

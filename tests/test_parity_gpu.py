@@ -182,3 +182,32 @@ def test_thin_disk_every_sample_written(renderer):
     disk = g.cls == 2
     assert np.allclose(g.cross[2, disk], np.pi / 2)
     assert np.isnan(g.cross[:, g.cls == 0]).all()
+
+
+# ---- full Dormand-Prince stepper (extension) --------------------------------
+def test_dp45_schwarzschild_256_full_parity(renderer, oracle_mod):
+    scene = workloads.schwarzschild_thin_256(stepper=abi.GG_STEPPER_DP45)
+    img, g = renderer.render(scene, rays=True)
+    oimg, o = oracle_mod.render(scene)
+    rep = compare(scene, g, o, oracle_mod)
+    assert rep["within_1e-9"] > 0.999, rep
+    assert (img == oimg).all(axis=2).mean() > 0.9999
+    assert (g.cls == 2).sum() > 1000
+
+
+def test_dp45_kerr_1080p_seeded_subset(renderer, oracle_mod):
+    scene = workloads.kerr_thin_1080p(stepper=abi.GG_STEPPER_DP45)
+    _, g = renderer.render(scene, rays=True)
+    idx = np.sort(np.random.default_rng(1).choice(scene.n_samples, 4096, replace=False))
+    o = oracle_mod.trace_samples(scene, idx.astype(np.uint64))
+    rep = compare(scene, g, o, oracle_mod, idx=idx.astype(np.int64))
+    assert rep["within_1e-9"] > 0.999, rep
+    # the crossing state (escape sphere / disk plane) from the Hermite interpolant
+    oc = oracle_mod.trace_cross(scene, idx.astype(np.uint64))
+    gc = g.cross[:, idx]
+    m = np.isfinite(oc[0]) & np.isfinite(gc[0])
+    assert m.sum() > 3000
+    d = np.abs(gc[:, m] - oc[:, m])
+    d[3] = np.abs(np.remainder(gc[3, m] - oc[3, m] + np.pi, 2 * np.pi) - np.pi)
+    rel = d.max(axis=0) / np.abs(oc[:, m]).max(axis=0)
+    assert np.quantile(rel, 0.999) < 1e-9, np.quantile(rel, 0.999)
