@@ -87,7 +87,8 @@ class gg_ray_out_t(C.Structure):
 
 class gg_stats_t(C.Structure):
     _fields_ = [("rays", C.c_uint64), ("attempts", C.c_uint64), ("accepted", C.c_uint64),
-                ("class_count", C.c_uint64 * 5), ("kernel_ms", C.c_double)]
+                ("class_count", C.c_uint64 * 5), ("kernel_ms", C.c_double),
+                ("fp64_rays", C.c_uint64), ("fp64_attempts", C.c_uint64)]
 
 
 STRUCTS = {

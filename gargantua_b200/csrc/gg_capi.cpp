@@ -33,6 +33,8 @@ struct gg_ctx {
   size_t samples_cap = 0;
   void* staging = nullptr;         // device outputs of the host-buffer entry point
   size_t staging_cap = 0;
+  void* queue = nullptr;           // mixed form: rays handed to the FP64 pass
+  size_t queue_cap = 0;
   bool pending = false;            // stats of the last device-pointer render not read yet
   gg_stats_t last{};
   std::mutex mu;
@@ -165,6 +167,19 @@ int validate(const gg_metric_t* metric, const gg_camera_t* camera, const gg_disk
   return GG_OK;
 }
 
+// Combinations the kernels implement beyond validate()'s field checks: the
+// mixed form runs the full Dormand-Prince stepper (the reference's step moves
+// positions by h*v_before, a first-order update whose endpoints follow the
+// exact step sequence, so FP32 rounding would show at 1e-4) with a thin disk
+// or none.
+int supported(const gg_disk_t* disk, const gg_integrator_t* integ) {
+  if (integ->precision == GG_PREC_MIXED) {
+    if (integ->stepper != GG_STEPPER_DP45) return GG_ERR_UNSUPPORTED;
+    if (disk && disk->kind == GG_DISK_VOLUMETRIC) return GG_ERR_UNSUPPORTED;
+  }
+  return GG_OK;
+}
+
 double photon_orbit(double mass, double spin) {
   return 2.0 * mass * (1.0 + std::cos((2.0 / 3.0) * std::acos(-spin / mass)));
 }
@@ -199,6 +214,18 @@ void build_params(const gg_metric_t* metric, const gg_camera_t* camera, const gg
   P.max_steps = integ->max_steps;
   P.precision = integ->precision;
   P.stepper = integ->stepper == GG_STEPPER_DP45 ? gg::kStepperDP45 : gg::kStepperReference;
+  P.mass_f = (float)P.mass;
+  P.spin_f = (float)P.spin;
+  P.rs_f = (float)P.rs;
+  P.atol_f = std::fmax((float)P.atol, 1.17549435e-38f);  // keep the scale of a 0 component > 0
+  P.rtol_f = (float)P.rtol;
+  P.max_radius_hi = (float)P.max_radius;
+  P.max_radius_lo = (float)(P.max_radius - (double)P.max_radius_hi);
+  // FP64 band: within 0.5 M of the prograde photon orbit or of the horizon
+  // test radius (the photon orbit lies outside the horizon), and 0.1 rad of
+  // the poles
+  P.band_r = (float)(std::fmax(P.r_photon, P.rh_plus_buffer) + 0.5);
+  P.pole_band = 0.1f;
 
   P.width = width;
   P.height = height;
@@ -292,15 +319,36 @@ int enqueue(gg_ctx* ctx, const DevParams& P, DevOutputs O, bool want_image,
     O.sample_rgb = nullptr;
   }
   if (!want_image) O.rgb8 = nullptr;
+  const bool mixed = P.precision == GG_PREC_MIXED;
+  O.queue = nullptr;
+  O.queue_cap = 0;
+  if (mixed) {  // every ray can be handed over at most once
+    const int st = grow(&ctx->queue, &ctx->queue_cap, sizeof(gg::QueuedRay) * P.n_rays);
+    if (st != GG_OK) return st;
+    O.queue = static_cast<gg::QueuedRay*>(ctx->queue);
+    O.queue_cap = P.n_rays;
+  }
   if (cudaMemsetAsync(ctx->ctl, 0, sizeof(DevControl), stream) != cudaSuccess) return GG_ERR_CUDA;
   int bps = 0;
-  if (gg::trace_occupancy(P, &bps) != cudaSuccess || bps < 1) return GG_ERR_CUDA;
+  const cudaError_t oe = mixed ? gg::mixed_occupancy(P, &bps) : gg::trace_occupancy(P, &bps);
+  if (oe != cudaSuccess || bps < 1) return GG_ERR_CUDA;
   uint64_t grid = (uint64_t)ctx->sms * (uint64_t)bps;
   const uint64_t need_blocks = (P.n_rays + gg::kTraceBlock - 1) / gg::kTraceBlock;
   if (grid > need_blocks) grid = need_blocks;
   if (grid < 1) grid = 1;
+  int qbps = 0;
+  if (mixed && (gg::queue_trace_occupancy(P, &qbps) != cudaSuccess || qbps < 1))
+    return GG_ERR_CUDA;
   if (cudaEventRecord(ctx->ev_start, stream) != cudaSuccess) return GG_ERR_CUDA;
-  if (gg::launch_trace(P, O, ctx->ctl, (int)grid, stream) != cudaSuccess) return GG_ERR_CUDA;
+  if (mixed) {
+    if (gg::launch_mixed(P, O, ctx->ctl, (int)grid, stream) != cudaSuccess) return GG_ERR_CUDA;
+    // the queue's length is only known on the device: a full persistent grid,
+    // whose surplus warps find the queue empty and exit
+    if (gg::launch_queue_trace(P, O, ctx->ctl, ctx->sms * qbps, stream) != cudaSuccess)
+      return GG_ERR_CUDA;
+  } else if (gg::launch_trace(P, O, ctx->ctl, (int)grid, stream) != cudaSuccess) {
+    return GG_ERR_CUDA;
+  }
   if (cudaEventRecord(ctx->ev_stop, stream) != cudaSuccess) return GG_ERR_CUDA;
   if (O.sample_rgb && O.rgb8) {
     if (gg::launch_reduce(P, O.sample_rgb, O.rgb8, ctx->sms, stream) != cudaSuccess)
@@ -327,9 +375,12 @@ int collect(gg_ctx* ctx) {
     s.class_count[k] = c.class_count[k];
     s.rays += c.class_count[k];
   }
+  s.fp64_rays = c.queued;
+  s.fp64_attempts = c.fp64_attempts;
   float ms = 0.f;
   if (cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop) == cudaSuccess) s.kernel_ms = ms;
   ctx->last = s;
+  if (c.queue_overflow) return GG_ERR_OOM;
   return c.abort ? GG_ERR_BUDGET : GG_OK;
 }
 
@@ -522,6 +573,7 @@ GG_API int gg_destroy(gg_ctx* c) {
   if (c->pending && c->ev_done) cudaEventSynchronize(c->ev_done);
   if (c->samples) cudaFree(c->samples);
   if (c->staging) cudaFree(c->staging);
+  if (c->queue) cudaFree(c->queue);
   if (c->ctl) cudaFree(c->ctl);
   if (c->ctl_host) cudaFreeHost(c->ctl_host);
   if (c->ev_start) cudaEventDestroy(c->ev_start);
@@ -556,7 +608,8 @@ GG_API int gg_render_device(gg_ctx* c, const gg_metric_t* metric, const gg_camer
   if (!c) return GG_ERR_INVALID_ARG;
   const int v = validate(metric, camera, disk, integ, opts, width, height);
   if (v != GG_OK) return v;
-  if (integ->precision != GG_PREC_FP64) return GG_ERR_UNSUPPORTED;
+  const int sup = supported(disk, integ);
+  if (sup != GG_OK) return sup;
   DevParams P;
   build_params(metric, camera, disk, integ, opts, width, height, &P);
   Lock lock(c);
@@ -586,7 +639,8 @@ GG_API int gg_render(gg_ctx* c, const gg_metric_t* metric, const gg_camera_t* ca
   if (!c) return GG_ERR_INVALID_ARG;
   const int v = validate(metric, camera, disk, integ, opts, width, height);
   if (v != GG_OK) return v;
-  if (integ->precision != GG_PREC_FP64) return GG_ERR_UNSUPPORTED;
+  const int sup = supported(disk, integ);
+  if (sup != GG_OK) return sup;
   DevParams P;
   build_params(metric, camera, disk, integ, opts, width, height, &P);
   Lock lock(c);

@@ -54,6 +54,12 @@ struct KerrGeo {
   T hrr, hthth;        // -g^rr / 2, -g^thth / 2
 };
 
+// 1/x: IEEE division in FP64; in the mixed form's FP32 right-hand side the
+// fast reciprocal (__fdividef, within 2 ulp), whose arguments there stay in
+// the normal range (r is outside the FP64 band, theta away from the poles).
+GG_DEV double rcp(double x) { return 1.0 / x; }
+GG_DEV float rcp(float x) { return __fdividef(1.0f, x); }
+
 template <class T>
 GG_DEV KerrGeo<T> kerr_geometry(T M, T a, T r, T s, T c) {
   KerrGeo<T> G;
@@ -62,7 +68,7 @@ GG_DEV KerrGeo<T> kerr_geometry(T M, T a, T r, T s, T c) {
   const T del = (r - T(2) * M) * r + a2;
   const T rho = r2 + a2;
   const T sd = sig * del;
-  const T R = T(1) / (sd * s2);
+  const T R = rcp(sd * s2);
   const T iSD = s2 * R;  // 1 / (Sigma Delta)
   const T iS = del * iSD;  // 1 / Sigma
   const T iD = sig * iSD;  // 1 / Delta
@@ -107,19 +113,22 @@ GG_DEV void kerr_contract(const KerrGeo<T>& G, const T v[4], T acc[4]) {
 }
 
 // Schwarzschild (schwarzschild.rs:99-140): 9 non-zero symbols, one reciprocal.
-struct SchwGeo {
-  double g_t_tr, g_r_tt, g_r_thth, g_r_phph, ir, g_th_phph, g_ph_thph;
+template <class T>
+struct SchwGeoT {
+  T g_t_tr, g_r_tt, g_r_thth, g_r_phph, ir, g_th_phph, g_ph_thph;
 };
+using SchwGeo = SchwGeoT<double>;
 
-GG_DEV SchwGeo schw_geometry(double rs, double r, double s, double c) {
-  SchwGeo G;
-  const double rmrs = r - rs;
-  const double R = 1.0 / (r * rmrs * s);  // 1 / (r (r - rs) sin)
-  const double ifd = s * R;                // 1 / (r (r - rs))
-  G.ir = rmrs * ifd;                       // 1 / r
-  const double is = (r * rmrs) * R;        // 1 / sin
-  G.g_t_tr = 0.5 * rs * ifd;
-  G.g_r_tt = 0.5 * rs * rmrs * (G.ir * G.ir * G.ir);
+template <class T>
+GG_DEV SchwGeoT<T> schw_geometry(T rs, T r, T s, T c) {
+  SchwGeoT<T> G;
+  const T rmrs = r - rs;
+  const T R = rcp(r * rmrs * s);  // 1 / (r (r - rs) sin)
+  const T ifd = s * R;            // 1 / (r (r - rs))
+  G.ir = rmrs * ifd;              // 1 / r
+  const T is = (r * rmrs) * R;    // 1 / sin
+  G.g_t_tr = T(0.5) * rs * ifd;
+  G.g_r_tt = T(0.5) * rs * rmrs * (G.ir * G.ir * G.ir);
   G.g_r_thth = -rmrs;
   G.g_r_phph = -rmrs * s * s;
   G.g_th_phph = -s * c;
@@ -127,13 +136,14 @@ GG_DEV SchwGeo schw_geometry(double rs, double r, double s, double c) {
   return G;
 }
 
-GG_DEV void schw_contract(const SchwGeo& G, const double v[4], double a[4]) {
-  const double vt = v[0], vr = v[1], vth = v[2], vph = v[3];
-  a[0] = -2.0 * G.g_t_tr * vt * vr;
+template <class T>
+GG_DEV void schw_contract(const SchwGeoT<T>& G, const T v[4], T a[4]) {
+  const T vt = v[0], vr = v[1], vth = v[2], vph = v[3];
+  a[0] = T(-2) * G.g_t_tr * vt * vr;
   a[1] = -G.g_r_tt * vt * vt + G.g_t_tr * vr * vr - G.g_r_thth * vth * vth -
          G.g_r_phph * vph * vph;
-  a[2] = -2.0 * G.ir * vr * vth - G.g_th_phph * vph * vph;
-  a[3] = -2.0 * G.ir * vr * vph - 2.0 * G.g_ph_thph * vth * vph;
+  a[2] = T(-2) * G.ir * vr * vth - G.g_th_phph * vph * vph;
+  a[3] = T(-2) * G.ir * vr * vph - T(2) * G.g_ph_thph * vth * vph;
 }
 
 template <int METRIC>
@@ -156,9 +166,9 @@ struct Geometry<kMetricSchwarzschild> {
   GG_DEV void at(const DevParams& P, double r, double th) {
     double s, c;
     sincos(th, &s, &c);
-    g = schw_geometry(P.rs, fmax(r, 1e-10), s, c);
+    g = schw_geometry<double>(P.rs, fmax(r, 1e-10), s, c);
   }
-  GG_DEV void accel(const double v[4], double a[4]) const { schw_contract(g, v, a); }
+  GG_DEV void accel(const double v[4], double a[4]) const { schw_contract<double>(g, v, a); }
 };
 
 template <int METRIC>

@@ -23,12 +23,29 @@ constexpr int kTraceMinBlocksKerr = 6;
 constexpr int kTraceMinBlocksSchw = 4;
 #endif
 
+// Resident CTAs per SM the mixed-precision trace kernel is budgeted for.
+#ifdef GG_MIXED_MIN_BLOCKS
+constexpr int kMixedMinBlocks = GG_MIXED_MIN_BLOCKS;
+#else
+constexpr int kMixedMinBlocks = 8;
+#endif
+
 // Resident CTAs per SM of the trace kernel `P` selects.
 cudaError_t trace_occupancy(const DevParams& P, int* blocks_per_sm);
 
 // Persistent trace over P.n_rays samples; `grid` CTAs of kTraceBlock threads.
 cudaError_t launch_trace(const DevParams& P, const DevOutputs& O, DevControl* ctl, int grid,
                          cudaStream_t stream);
+
+// Mixed form (P.precision == GG_PREC_MIXED, full Dormand-Prince): the FP32
+// pass over the samples, which hands FP64-band rays to O.queue, and the FP64
+// pass over that queue.
+cudaError_t mixed_occupancy(const DevParams& P, int* blocks_per_sm);
+cudaError_t launch_mixed(const DevParams& P, const DevOutputs& O, DevControl* ctl, int grid,
+                         cudaStream_t stream);
+cudaError_t queue_trace_occupancy(const DevParams& P, int* blocks_per_sm);
+cudaError_t launch_queue_trace(const DevParams& P, const DevOutputs& O, DevControl* ctl,
+                               int grid, cudaStream_t stream);
 
 // Best-of-5 FMA throughput (FLOP/s, FMA = 2) of the current device.
 cudaError_t measure_fma_peak(int fp64, int sms, double* flops);

@@ -1,0 +1,333 @@
+// gg_mixed.cu -- the mixed-precision persistent trace kernel (GG_PREC_MIXED).
+//
+// Same work decomposition as the FP64 kernel (gg_trace.cu): persistent CTAs,
+// 32-sample chunks per warp, ballot refill every kPeriod attempts.  Each lane
+// steps its ray with the mixed-precision full Dormand-Prince attempt
+// (gg_mixed.cuh).  When a ray's next attempt would start inside the FP64
+// band -- r within 0.5 M of the horizon (with its buffer) or of the prograde
+// photon orbit, theta within pole_band of a pole, or a step that would carry
+// theta across a pole -- the lane writes the ray's state, in FP64, to a
+// global queue and takes a new sample.  The FP64 kernel then runs over that
+// queue in a second launch (trace_fp64_kernel<..., kSrcQueue>).  Handing rays
+// off instead of running FP64 attempts inside this kernel keeps both launches
+// warp-uniform: a warp never executes the FP32 and the FP64 attempt
+// back to back for lanes in different bands.
+//
+// Crossings of the escape sphere and the disk plane are detected on the
+// float-pair differences and located in FP64 on the step's cubic Hermite
+// interpolant, as in the FP64 kernel.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "gg_device.cuh"
+#include "gg_launch.h"
+#include "gg_mixed.cuh"
+#include "gg_trace_common.cuh"
+
+namespace gg {
+
+namespace {
+
+// Writes the ray to the FP64 pass's queue (out of line: once per handed-off
+// ray).  The state is the one the next attempt starts from.  The register
+// part of the ray comes by value, so the stepping loop keeps it in registers.
+__device__ __noinline__ void hand_off(const DevOutputs& O, DevControl* ctl, MixedSmem K,
+                                      MixedRegs S, uint32_t n_att, uint32_t n_acc) {
+  const unsigned long long slot = atomicAdd(&ctl->queued, 1ull);
+  if (slot >= O.queue_cap) {
+    atomicExch(&ctl->queue_overflow, 1u);
+    return;
+  }
+  const Ray R = mixed_fp64(K, S);
+  QueuedRay& q = O.queue[slot];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    q.x[i] = R.x[i];
+    q.v[i] = R.v[i];
+  }
+  q.h = R.h;
+  q.lam = R.lam;
+  q.idx = K.idx();
+  q.n_att = n_att;
+  q.n_acc = n_acc;
+}
+
+// Writes a finished ray's outcome (its state converted to FP64) and counts it
+// in the block's statistics.  Out of line, once per ray.
+__device__ __noinline__ void mixed_finish(const DevParams& P, const DevOutputs& O, MixedSmem K,
+                                          MixedRegs S, int cls, uint32_t n_att, uint32_t n_acc,
+                                          bool crossed, BlockStats* bs) {
+  finish_sample(P, O, K.idx(), cls, mixed_fp64(K, S), n_att, n_acc, 0.0, 0.0, crossed);
+  atomicAdd(&bs->attempts, (unsigned long long)n_att);
+  atomicAdd(&bs->accepted, (unsigned long long)n_acc);
+  atomicAdd(&bs->cls[cls], 1ull);
+}
+
+// The accepted step (pre-step state, increments in slots 7, 8, k1 in slot
+// 0, k7 in slot 6) crossed the escape sphere (`esc`) and/or the disk
+// plane (`dsk`): locate the crossings in FP64 on the Hermite interpolant.
+// Stores the escape crossing; when the ray ends on the thin disk, writes its
+// outcome at the crossing and returns true.
+template <int METRIC, int DISK>
+__device__ __noinline__ bool mixed_crossings(const DevParams& P, const DevOutputs& O, MixedSmem K,
+                                             MixedRegs S, float hf, bool esc, bool dsk,
+                                             uint32_t n_att, uint32_t n_acc, BlockStats* bs) {
+  const Ray B = mixed_fp64(K, S);
+  const uint64_t idx = K.idx();
+  const float4 dx4 = K.get(kSlotDx), dv4 = K.get(kSlotDv), k14 = K.get(0), k74 = K.get(6);
+  const float dx[4] = {dx4.x, dx4.y, dx4.z, dx4.w}, dv[4] = {dv4.x, dv4.y, dv4.z, dv4.w};
+  const float k1[4] = {k14.x, k14.y, k14.z, k14.w}, k7[4] = {k74.x, k74.y, k74.z, k74.w};
+  double xa[4], va[4], kb[4], ka[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    xa[i] = B.x[i] + (double)dx[i];
+    va[i] = B.v[i] + (double)dv[i];
+    kb[i] = (double)k1[i];
+    ka[i] = (double)k7[i];
+  }
+  const double h = (double)hf;
+  if (esc && O.cross) {
+    const double s = hermite_root(B.x, B.v, xa, va, h, 1, P.max_radius);
+    double c[8];
+    hermite_point(B.x, B.v, kb, xa, va, ka, h, s, c);
+    normalize_coords(c);
+    store_cross(P, O, idx, c);
+  }
+  if (DISK == kDiskThin && dsk) {
+    const double s = hermite_root(B.x, B.v, xa, va, h, 2, kHalfPi);
+    double c[8];
+    hermite_point(B.x, B.v, kb, xa, va, ka, h, s, c);
+    normalize_coords(c);
+    const double r_c = c[1];
+    if (r_c >= P.r_inner && r_c <= P.r_outer) {
+      c[2] = kHalfPi;
+      const double g = redshift_factor<METRIC>(P, r_c, kHalfPi, c + 4);
+      const double q = P.r_inner / r_c;
+      const double g2 = g * g;
+      Ray end;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        end.x[i] = c[i];
+        end.v[i] = c[4 + i];
+      }
+      end.h = S.h;
+      end.lam = B.lam + s * h;
+      store_cross(P, O, idx, c);
+      finish_sample(P, O, idx, kClsDisk, end, n_att, n_acc, (g2 * g2) * pow(q, P.emissivity_index),
+                    g * pow(q, 0.75), true);
+      atomicAdd(&bs->attempts, (unsigned long long)n_att);
+      atomicAdd(&bs->accepted, (unsigned long long)n_acc);
+      atomicAdd(&bs->cls[kClsDisk], 1ull);
+      return true;
+    }
+  }
+  return false;
+}
+
+// BUDGET: the render has an attempt budget (its bookkeeping costs registers,
+// so renders without one run a variant that has none).
+template <int METRIC, int DISK, bool BUDGET>
+__global__ void __launch_bounds__(kTraceBlock, kMixedMinBlocks)
+    trace_mixed_kernel(const __grid_constant__ DevParams P, const __grid_constant__ DevOutputs O,
+                       DevControl* ctl) {
+  const unsigned lane = threadIdx.x & 31u;
+  __shared__ BlockStats bs;
+  __shared__ float4 k_smem[kMixedSlots][kTraceBlock];
+  __shared__ double lam_smem[kTraceBlock];
+  __shared__ uint64_t idx_smem[kTraceBlock];
+  const MixedSmem K{k_smem, lam_smem, idx_smem};
+  if (threadIdx.x < sizeof(BlockStats) / 8)
+    reinterpret_cast<unsigned long long*>(&bs)[threadIdx.x] = 0ull;
+  __syncthreads();
+
+  MixedRegs S;
+  bool live = false;
+  uint32_t n_att = 0, n_acc = 0;
+  bool crossed = false;
+  bool k1_valid = false;
+  bool k7_pending = false;
+
+  uint64_t wbase = 0;
+  uint32_t wcount = 0;
+  bool wdone = false;
+  unsigned budget_pending = 0;
+
+  for (;;) {
+    // ---- refill lanes whose ray finished or was handed off ----------------
+    unsigned need = __ballot_sync(kFull, !live);
+    if (BUDGET && need && !wdone) {
+      unsigned long long ab = 0;
+      if (lane == 0) ab = atomicOr(&ctl->abort, 0u);
+      if (__shfl_sync(kFull, ab, 0)) wdone = true;
+    }
+    while (need && !wdone) {
+      if (wcount == 0) {
+        unsigned long long b = 0;
+        if (lane == 0) {
+          b = atomicAdd(&ctl->next_ray, (unsigned long long)kChunk);
+          if (BUDGET) {
+            const unsigned long long used = atomicAdd(&ctl->budget_used, 0ull);
+            if (used > P.attempt_budget) {
+              atomicExch(&ctl->abort, 1u);
+              b = P.n_rays;
+            }
+          }
+        }
+        b = __shfl_sync(kFull, b, 0);
+        if (b >= P.n_rays) {
+          wdone = true;
+          break;
+        }
+        wbase = b;
+        const uint64_t left = P.n_rays - b;
+        wcount = left < kChunk ? (uint32_t)left : kChunk;
+      }
+      const unsigned nn = (unsigned)__popc(need);
+      const unsigned take = nn < wcount ? nn : wcount;
+      const unsigned rank = (unsigned)__popc(need & lanemask_lt());
+      if (!live && rank < take) {
+        const uint64_t idx = wbase + rank;
+        mixed_load(start_sample(P, idx), idx, K, S);
+        live = true;
+        n_att = 0;
+        n_acc = 0;
+        crossed = false;
+        k1_valid = false;
+        k7_pending = false;
+      }
+      wbase += take;
+      wcount -= take;
+      need = __ballot_sync(kFull, !live);
+    }
+    if (!__any_sync(kFull, live)) break;
+
+    // ---- advance every live ray by up to kPeriod attempts -----------------
+#pragma unroll 1
+    for (int it = 0; it < kPeriod; ++it) {
+      if (!live) continue;
+      {
+        const float r = K.comp(kSlotXh, 1), th = K.comp(kSlotXh, 2);
+        if (r < P.band_r || th < P.pole_band || th > kPiHi - P.pole_band) {
+          hand_off(O, ctl, K, S, n_att, n_acc);
+          live = false;
+          continue;
+        }
+      }
+      bool acc;
+      float hf = 0.0f;
+      const int res = attempt_dp45_mixed<METRIC>(P, S, K, k1_valid, k7_pending, acc, hf);
+      n_att += 1;
+      int done_cls = -1;
+      if (acc) {
+        const float4 dx = K.get(kSlotDx);
+        const float4 xh = K.get(kSlotXh), xl = K.get(kSlotXl);
+        const float th_a = xh.z + dx.z;
+        if (!(th_a > 0.0f && th_a < kPiHi)) {
+          // theta would turn through a pole: re-take this step in FP64
+          n_att -= 1;
+          hand_off(O, ctl, K, S, n_att, n_acc);
+          live = false;
+          continue;
+        }
+        n_acc += 1;
+        const float dr_b = ff_minus(xh.y, xl.y, P.max_radius_hi, P.max_radius_lo);
+        const bool esc = dr_b <= 0.0f && dr_b + dx.y > 0.0f;
+        bool dsk = false;
+        if (DISK == kDiskThin) {
+          const float d_b = ff_minus(xh.z, xl.z, kHalfPiHi, kHalfPiLo);
+          const float d_a = d_b + dx.z;
+          dsk = (d_b < 0.0f && d_a >= 0.0f) || (d_b > 0.0f && d_a <= 0.0f);
+        }
+        if (esc || dsk) {
+          if (esc && O.cross) crossed = true;
+          if (mixed_crossings<METRIC, DISK>(P, O, K, S, hf, esc, dsk, n_att, n_acc, &bs)) {
+            if (BUDGET) budget_pending += n_att;
+            live = false;
+            continue;
+          }
+        }
+        mixed_advance(S, K, hf, k1_valid, k7_pending);
+      }
+      if (res == kEscaped) done_cls = kClsEscaped;
+      else if (n_att >= P.max_steps) done_cls = kClsMaxSteps;
+      if (done_cls >= 0) {
+        mixed_finish(P, O, K, S, done_cls, n_att, n_acc, crossed, &bs);
+        if (BUDGET) budget_pending += n_att;
+        live = false;
+      }
+    }
+    if (BUDGET) {
+      const unsigned long long wsum = __reduce_add_sync(kFull, budget_pending);
+      budget_pending = 0;
+      unsigned ab = 0;
+      if (lane == 0) {
+        const unsigned long long used = atomicAdd(&ctl->budget_used, wsum) + wsum;
+        if (used > P.attempt_budget) atomicExch(&ctl->abort, 1u);
+        ab = atomicOr(&ctl->abort, 0u);
+      }
+      if (__shfl_sync(kFull, ab, 0)) {
+        wdone = true;
+        if (live) {
+          mixed_finish(P, O, K, S, kClsBudget, n_att, n_acc, crossed, &bs);
+          live = false;
+        }
+      }
+    }
+  }
+
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    atomicAdd(&ctl->attempts, bs.attempts);
+    atomicAdd(&ctl->accepted, bs.accepted);
+#pragma unroll
+    for (int k = 0; k < 5; ++k)
+      if (bs.cls[k]) atomicAdd(&ctl->class_count[k], bs.cls[k]);
+  }
+}
+
+template <int METRIC, int DISK, bool BUDGET>
+const void* mixed_fn() {
+  return reinterpret_cast<const void*>(&trace_mixed_kernel<METRIC, DISK, BUDGET>);
+}
+
+template <bool BUDGET>
+const void* select_mixed_disk(const DevParams& P) {
+  if (P.metric == kMetricKerr)
+    return P.disk == kDiskThin ? mixed_fn<kMetricKerr, kDiskThin, BUDGET>()
+                               : mixed_fn<kMetricKerr, kDiskNone, BUDGET>();
+  return P.disk == kDiskThin ? mixed_fn<kMetricSchwarzschild, kDiskThin, BUDGET>()
+                             : mixed_fn<kMetricSchwarzschild, kDiskNone, BUDGET>();
+}
+
+const void* select_mixed(const DevParams& P) {
+  return P.attempt_budget ? select_mixed_disk<true>(P) : select_mixed_disk<false>(P);
+}
+
+}  // namespace
+
+cudaError_t mixed_occupancy(const DevParams& P, int* blocks_per_sm) {
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, select_mixed(P),
+                                                       kTraceBlock, 0);
+}
+
+cudaError_t launch_mixed(const DevParams& P, const DevOutputs& O, DevControl* ctl, int grid,
+                         cudaStream_t stream) {
+  const void* fn = select_mixed(P);
+  DevParams p = P;
+  DevOutputs o = O;
+  void* args[] = {&p, &o, &ctl};
+  return cudaLaunchKernel(fn, dim3(grid), dim3(kTraceBlock), args, 0, stream);
+}
+
+}  // namespace gg
+
+// The mixed kernel's polar-angle sincos evaluated on the host from the same
+// source, so tests can check it against a double-precision reference.
+extern "C" __attribute__((visibility("default"))) int gg_polar_sincos(const float* theta,
+                                                                       float* s, float* c,
+                                                                       uint32_t n) {
+  if (!theta || !s || !c) return -1;
+  for (uint32_t i = 0; i < n; ++i) gg::sincos_polar(theta[i], s + i, c + i);
+  return 0;
+}

@@ -1,0 +1,391 @@
+// gg_mixed.cuh -- the mixed-precision form of the full Dormand-Prince step.
+//
+// Where the precision goes.  The ray state (x, v) is a pair of floats per
+// component, hi + lo (about 48 significant bits), and each accepted step adds
+// its FP32 increment to it with a compensated (two-sum) addition: without
+// that, rounding the state to FP32 every step would cost eps * |x| per step,
+// 1e-5 M at r = 200 after a few hundred steps.  Everything that is small
+// relative to the state runs in FP32: the stage positions and velocities
+// (formed as increments over the state), the seven right-hand sides, and the
+// embedded error estimate, which the Nystrom form builds directly from the
+// stage derivatives (weights c - d), so it carries no cancellation.  The
+// error norm's final reduction and the step-size controller (acceptance test,
+// fifth root, clamps, the step h itself) are FP64.  Attempts that start within
+// 0.5 M of the horizon or of the prograde photon orbit, or near a pole (where
+// Boyer-Lindquist theta turns and is reflected), run in the FP64 pass: the
+// ray is handed over with its state converted to FP64 (gg_mixed.cu).
+//
+// Where the state lives.  Registers hold only what every stage reads: the
+// velocity's hi part and the FP64 step.  The position pair, the velocity's
+// lo part, the affine parameter and the sample index live in this lane's
+// column of shared memory (MixedSmem), read once per attempt and written
+// once per accepted step, which keeps the stepping loop within 64 registers
+// without spilling.  The right-hand side depends on (r, theta, v) only -- the
+// metric is stationary and axisymmetric -- so stages form r and theta alone;
+// the t and phi increments are formed once, for the accepted step.
+#pragma once
+
+#include "gg_device.cuh"
+
+namespace gg {
+
+constexpr float kPiHi = 3.14159274101257324f;  // float(pi), rounded up
+constexpr float kPiLo = -8.74227765734758577e-08f;  // pi - kPiHi
+constexpr float kHalfPiHi = 1.57079637050628662f;
+constexpr float kHalfPiLo = -4.37113882867379300e-08f;  // pi/2 - kHalfPiHi
+constexpr float kTwoPiHi = 6.28318548202514648f;
+constexpr float kTwoPiLo = -1.74845553146951720e-07f;  // 2 pi - kTwoPiHi
+constexpr float kQuarterPiF = 0.785398163397448310f;
+
+// sin and cos of a Boyer-Lindquist polar angle, for theta in [-pi/4, 5pi/4]:
+// reduce to |u| <= pi/4 about 0, pi/2 or pi (the reductions about pi/2 and pi
+// subtract the float pair of the constant, exactly in its leading part by
+// Sterbenz), then the Taylor series of sin u to u^9 and of cos u to u^10
+// (truncation below 2e-9 on |u| <= pi/4), Horner with fused multiply-adds.
+// Branch-free; the same source runs on the host for testing.
+__host__ __device__ __forceinline__ void sincos_polar(float th, float* s_out, float* c_out) {
+  const bool lo_q = th < kQuarterPiF;
+  const bool hi_q = th > 3.0f * kQuarterPiF;
+  const float u_mid = (th - kHalfPiHi) - kHalfPiLo;  // theta = pi/2 + u
+  const float u_top = (kPiHi - th) + kPiLo;          // theta = pi - u
+  const float u = lo_q ? th : (hi_q ? u_top : u_mid);
+  const float u2 = u * u;
+  float ps = fmaf(u2, 1.0f / 362880.0f, -1.0f / 5040.0f);
+  ps = fmaf(u2, ps, 1.0f / 120.0f);
+  ps = fmaf(u2, ps, -1.0f / 6.0f);
+  ps = u2 * ps;
+  const float su = fmaf(u, ps, u);
+  float pc = fmaf(u2, -1.0f / 3628800.0f, 1.0f / 40320.0f);
+  pc = fmaf(u2, pc, -1.0f / 720.0f);
+  pc = fmaf(u2, pc, 1.0f / 24.0f);
+  pc = fmaf(u2, pc, -0.5f);
+  const float cu = fmaf(u2, pc, 1.0f);
+  *s_out = lo_q ? su : (hi_q ? su : cu);
+  *c_out = lo_q ? cu : (hi_q ? -cu : -su);
+}
+
+// hi + lo += d: two-sum of hi and d (exact), its rounding error folded into
+// lo, then renormalised so that |lo| <= ulp(hi) / 2.
+GG_DEV void ff_add(float& hi, float& lo, float d) {
+  const float s = hi + d;
+  const float bb = s - hi;
+  const float e = (hi - (s - bb)) + (d - bb);
+  const float t = lo + e;
+  hi = s + t;
+  lo = t - (hi - s);
+}
+
+// (hi + lo) - (c_hi + c_lo) to FP32 accuracy, exact in its leading part when
+// hi is within a factor 2 of c_hi (Sterbenz): the sign tests of the escape
+// sphere and the disk plane are made on this difference.
+GG_DEV float ff_minus(float hi, float lo, float c_hi, float c_lo) {
+  return (hi - c_hi) + (lo - c_lo);
+}
+
+GG_DEV void split(double x, float& hi, float& lo) {
+  hi = (float)x;
+  lo = (float)(x - (double)hi);
+}
+
+// This lane's column of the mixed kernel's shared memory: float4 slots
+// [slot][thread] (a warp's 16-byte accesses are conflict-free), plus the
+// affine parameter and sample index.  Slots 0-6 hold k1..k7 (k7 = a at the
+// new state, the next attempt's k1); 7 and 8 the accepted step's increments
+// dx, dv; 9 and 10 the position hi and lo parts; 11 the velocity lo part.
+constexpr int kSlotDx = 7, kSlotDv = 8, kSlotXh = 9, kSlotXl = 10, kSlotVl = 11;
+constexpr int kMixedSlots = 12;
+struct MixedSmem {
+  float4 (*s)[kTraceBlock];
+  double* lam_s;
+  uint64_t* idx_s;
+  GG_DEV float4 get(int slot) const { return s[slot][threadIdx.x]; }
+  GG_DEV void set(int slot, float4 v) const { s[slot][threadIdx.x] = v; }
+  GG_DEV float comp(int slot, int i) const {
+    return reinterpret_cast<const float*>(&s[slot][threadIdx.x])[i];
+  }
+  GG_DEV double& lam() const { return lam_s[threadIdx.x]; }
+  GG_DEV uint64_t& idx() const { return idx_s[threadIdx.x]; }
+};
+
+// Register part of a mixed-form ray.
+struct MixedRegs {
+  float vh[4];  // velocity, hi part
+  double h;     // step size (controller state, FP64)
+};
+
+// Starts a ray: state from FP64, split into hi + lo.
+GG_DEV void mixed_load(const Ray& R, uint64_t idx, const MixedSmem& K, MixedRegs& S) {
+  float xh[4], xl[4], vl[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    split(R.x[i], xh[i], xl[i]);
+    split(R.v[i], S.vh[i], vl[i]);
+  }
+  K.set(kSlotXh, make_float4(xh[0], xh[1], xh[2], xh[3]));
+  K.set(kSlotXl, make_float4(xl[0], xl[1], xl[2], xl[3]));
+  K.set(kSlotVl, make_float4(vl[0], vl[1], vl[2], vl[3]));
+  K.lam() = R.lam;
+  K.idx() = idx;
+  S.h = R.h;
+}
+
+// The ray's state in FP64 (hi + lo).
+GG_DEV Ray mixed_fp64(const MixedSmem& K, const MixedRegs& S) {
+  const float4 xh = K.get(kSlotXh), xl = K.get(kSlotXl), vl = K.get(kSlotVl);
+  Ray R;
+  R.x[0] = (double)xh.x + (double)xl.x;
+  R.x[1] = (double)xh.y + (double)xl.y;
+  R.x[2] = (double)xh.z + (double)xl.z;
+  R.x[3] = (double)xh.w + (double)xl.w;
+  R.v[0] = (double)S.vh[0] + (double)vl.x;
+  R.v[1] = (double)S.vh[1] + (double)vl.y;
+  R.v[2] = (double)S.vh[2] + (double)vl.z;
+  R.v[3] = (double)S.vh[3] + (double)vl.w;
+  R.h = S.h;
+  R.lam = K.lam();
+  return R;
+}
+
+// Dormand-Prince coefficients as FP32 compile-time constants, so the unrolled
+// stage sums fold them into the FMAs and drop the zero ones.
+template <int S, int L>
+struct DPc {
+  static constexpr float abar = static_cast<float>(make_dp_table().Abar[S][L]);
+  static constexpr float b = static_cast<float>(make_dp_table().B[S][L]);
+};
+template <int L>
+struct DPe {
+  static constexpr float e = static_cast<float>(make_dp_table().E[L]);
+  static constexpr float ebar = static_cast<float>(make_dp_table().Ebar[L]);
+};
+template <int S>
+struct DPa {
+  static constexpr float a = static_cast<float>(make_dp_table().A[S]);
+};
+
+// ax += sum_l Abar[S][l] k_l, av += sum_l B[S][l] k_l over l < S.
+template <int S, int L>
+GG_DEV void stage_sums(const MixedSmem& K, float ax[4], float av[4]) {
+  if constexpr (L < S) {
+    constexpr float cb = DPc<S, L>::abar, cv = DPc<S, L>::b;
+    if constexpr (cb != 0.0f || cv != 0.0f) {
+      const float4 k4 = K.get(L);
+      const float k[4] = {k4.x, k4.y, k4.z, k4.w};
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        if constexpr (cb != 0.0f) ax[i] = fmaf(cb, k[i], ax[i]);
+        if constexpr (cv != 0.0f) av[i] = fmaf(cv, k[i], av[i]);
+      }
+    }
+    stage_sums<S, L + 1>(K, ax, av);
+  }
+}
+
+// ex += sum_l Ebar_l k_l, ev += sum_l E_l k_l over the seven stages.
+template <int L>
+GG_DEV void error_sums(const MixedSmem& K, float ex[4], float ev[4]) {
+  if constexpr (L < 7) {
+    constexpr float eb = DPe<L>::ebar, e = DPe<L>::e;
+    if constexpr (eb != 0.0f || e != 0.0f) {
+      const float4 k4 = K.get(L);
+      const float k[4] = {k4.x, k4.y, k4.z, k4.w};
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        if constexpr (eb != 0.0f) ex[i] = fmaf(eb, k[i], ex[i]);
+        if constexpr (e != 0.0f) ev[i] = fmaf(e, k[i], ev[i]);
+      }
+    }
+    error_sums<L + 1>(K, ex, ev);
+  }
+}
+
+// Stage S's r, theta and velocity as increments over the state's hi part:
+// x_S = x + h a_S v + h^2 sum Abar k, v_S = v + h sum B k.  Stage 6 is the
+// 5th-order solution: its four position and velocity increments are the
+// step's dx, dv (slots 7, 8).
+template <int S>
+GG_DEV void mixed_stage(float r0, float th0, const MixedRegs& st, const MixedSmem& K, float hf,
+                        float hh, float& pr, float& pth, float pw[4]) {
+  float ax[4] = {0.0f, 0.0f, 0.0f, 0.0f}, av[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+  stage_sums<S, 0>(K, ax, av);
+  const float ha = hf * DPa<S>::a;
+  float dx[4], dv[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    dx[i] = fmaf(hh, ax[i], ha * st.vh[i]);
+    dv[i] = hf * av[i];
+    pw[i] = st.vh[i] + dv[i];
+  }
+  pr = r0 + dx[1];
+  pth = th0 + dx[2];
+  if constexpr (S == 6) {
+    K.set(kSlotDx, make_float4(dx[0], dx[1], dx[2], dx[3]));
+    K.set(kSlotDv, make_float4(dv[0], dv[1], dv[2], dv[3]));
+  }
+}
+
+template <int METRIC>
+struct Geometry32;
+
+template <>
+struct Geometry32<kMetricKerr> {
+  KerrGeo<float> g;
+  GG_DEV void at(const DevParams& P, float r, float th) {
+    float s, c;
+    sincos_polar(th, &s, &c);
+    g = kerr_geometry<float>(P.mass_f, P.spin_f, fmaxf(r, 1e-10f), s, c);
+  }
+  GG_DEV void accel(const float v[4], float a[4]) const { kerr_contract<float>(g, v, a); }
+};
+
+template <>
+struct Geometry32<kMetricSchwarzschild> {
+  SchwGeoT<float> g;
+  GG_DEV void at(const DevParams& P, float r, float th) {
+    float s, c;
+    sincos_polar(th, &s, &c);
+    g = schw_geometry<float>(P.rs_f, fmaxf(r, 1e-10f), s, c);
+  }
+  GG_DEV void accel(const float v[4], float a[4]) const { schw_contract<float>(g, v, a); }
+};
+
+// x^(1/5) for x in (1, 1e30], larger x taken as 1e30: on acceptance
+// x = tol/err > 1, and a root above 1e6 only matters through the max_step
+// clamp.  Same seed-and-Newton scheme as fifth_root, without its pow branch.
+GG_DEV double fifth_root_accept(double x) {
+  x = fmin(x, 1e30);
+  double z = (double)__powf((float)x, -0.2f);
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const double z2 = z * z;
+    z = z * (1.2 - 0.2 * x * (z2 * z2 * z));
+  }
+  const double z2 = z * z;
+  return x * (z2 * z2);
+}
+
+// The escape test of the reference's step (geodesic.rs:195-197) on the
+// float-pair radius.
+GG_DEV bool beyond_max_radius(const DevParams& P, const MixedSmem& K) {
+  return ff_minus(K.comp(kSlotXh, 1), K.comp(kSlotXl, 1), P.max_radius_hi, P.max_radius_lo) >
+         0.0f;
+}
+
+// One mixed-precision attempt of the full Dormand-Prince step.  Control flow
+// is attempt_dp45_fp64's: escape test, invalid-stage halving, acceptance test
+// and step-size law (FP64).  On acceptance the state is NOT advanced: the
+// increments are in slots 7 and 8 and hf is the step taken, so the caller
+// can test the step for crossings against the pre-step state first
+// (mixed_advance applies it).  The horizon test never fires here: the FP64
+// band starts 0.5 M outside the horizon and its buffer.  Invalid stages are
+// judged on r and theta, the coordinates the stages form.
+template <int METRIC>
+GG_DEV int attempt_dp45_mixed(const DevParams& P, MixedRegs& S, const MixedSmem& K,
+                              bool& k1_valid, bool& k7_pending, bool& accepted, float& hf) {
+  accepted = false;
+  if (beyond_max_radius(P, K)) return kEscaped;
+  if (k7_pending) {
+    K.set(0, K.get(6));
+    k7_pending = false;
+  }
+  hf = (float)S.h;
+  const float hh = hf * hf;
+  const float r0 = K.comp(kSlotXh, 1), th0 = K.comp(kSlotXh, 2);
+  const int s_first = __any_sync(__activemask(), !k1_valid) ? 0 : 1;
+#pragma unroll 1
+  for (int s = s_first; s < 7; ++s) {
+    float pr, pth, pw[4];
+    switch (s) {
+      case 0:
+        pr = r0;
+        pth = th0;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) pw[i] = S.vh[i];
+        break;
+      case 1: mixed_stage<1>(r0, th0, S, K, hf, hh, pr, pth, pw); break;
+      case 2: mixed_stage<2>(r0, th0, S, K, hf, hh, pr, pth, pw); break;
+      case 3: mixed_stage<3>(r0, th0, S, K, hf, hh, pr, pth, pw); break;
+      case 4: mixed_stage<4>(r0, th0, S, K, hf, hh, pr, pth, pw); break;
+      case 5: mixed_stage<5>(r0, th0, S, K, hf, hh, pr, pth, pw); break;
+      default: mixed_stage<6>(r0, th0, S, K, hf, hh, pr, pth, pw); break;
+    }
+    if (s > 0 && !(isfinite(pr) && isfinite(pth) && pr > 0.0f)) {
+      S.h = S.h * 0.5;
+      return kContinue;
+    }
+    Geometry32<METRIC> G;
+    G.at(P, pr, pth);
+    float a[4];
+    G.accel(pw, a);
+    K.set(s, make_float4(a[0], a[1], a[2], a[3]));
+  }
+  float ex[4] = {0.0f, 0.0f, 0.0f, 0.0f}, ev[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+  error_sums<0>(K, ex, ev);
+  const float4 dx4 = K.get(kSlotDx), dv4 = K.get(kSlotDv), xh4 = K.get(kSlotXh);
+  const float dx[4] = {dx4.x, dx4.y, dx4.z, dx4.w}, dv[4] = {dv4.x, dv4.y, dv4.z, dv4.w};
+  const float xh[4] = {xh4.x, xh4.y, xh4.z, xh4.w};
+  float s2 = 0.0f;
+  double err, tol;
+  if (P.rtol > 0.0) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const float xs = fmaf(P.rtol_f, fmaxf(fabsf(xh[i]), fabsf(xh[i] + dx[i])), P.atol_f);
+      const float vs = fmaf(P.rtol_f, fmaxf(fabsf(S.vh[i]), fabsf(S.vh[i] + dv[i])), P.atol_f);
+      const float qx = __fdividef(hh * ex[i], xs);
+      const float qv = __fdividef(hf * ev[i], vs);
+      s2 = fmaf(qx, qx, fmaf(qv, qv, s2));
+    }
+    err = sqrt((double)s2 * 0.125);
+    tol = 1.0;
+  } else {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const float ax = hh * ex[i], av = hf * ev[i];
+      s2 = fmaf(ax, ax, fmaf(av, av, s2));
+    }
+    err = sqrt((double)s2);
+    tol = P.tolerance;
+  }
+  if (err < tol || S.h <= P.min_step) {
+    accepted = true;
+    if (err > 0.0) {
+      double hn = S.h * 0.9 * fifth_root_accept(tol / err);
+      hn = hn < P.min_step ? P.min_step : (hn > P.max_step ? P.max_step : hn);
+      S.h = hn;
+    }
+  } else {
+    S.h = fmax(S.h * 0.9 * sqrt(sqrt(tol / err)), P.min_step);
+  }
+  return kContinue;
+}
+
+// Applies an accepted attempt's increments (compensated) and wraps phi into
+// [0, 2 pi); k7 becomes the next attempt's k1.
+GG_DEV void mixed_advance(MixedRegs& S, const MixedSmem& K, float hf, bool& k1_valid,
+                          bool& k7_pending) {
+  const float4 dx4 = K.get(kSlotDx), dv4 = K.get(kSlotDv);
+  const float4 xh4 = K.get(kSlotXh), xl4 = K.get(kSlotXl), vl4 = K.get(kSlotVl);
+  float xh[4] = {xh4.x, xh4.y, xh4.z, xh4.w}, xl[4] = {xl4.x, xl4.y, xl4.z, xl4.w};
+  float vl[4] = {vl4.x, vl4.y, vl4.z, vl4.w};
+  const float dx[4] = {dx4.x, dx4.y, dx4.z, dx4.w}, dv[4] = {dv4.x, dv4.y, dv4.z, dv4.w};
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    ff_add(xh[i], xl[i], dx[i]);
+    ff_add(S.vh[i], vl[i], dv[i]);
+  }
+  if (xh[3] >= kTwoPiHi) {
+    ff_add(xh[3], xl[3], -kTwoPiHi);
+    ff_add(xh[3], xl[3], -kTwoPiLo);
+  } else if (xh[3] < 0.0f) {
+    ff_add(xh[3], xl[3], kTwoPiHi);
+    ff_add(xh[3], xl[3], kTwoPiLo);
+  }
+  K.set(kSlotXh, make_float4(xh[0], xh[1], xh[2], xh[3]));
+  K.set(kSlotXl, make_float4(xl[0], xl[1], xl[2], xl[3]));
+  K.set(kSlotVl, make_float4(vl[0], vl[1], vl[2], vl[3]));
+  K.lam() = K.lam() + (double)hf;
+  k1_valid = true;
+  k7_pending = true;
+}
+
+}  // namespace gg

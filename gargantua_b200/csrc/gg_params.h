@@ -32,6 +32,13 @@ struct DevParams {
   int precision;
   int stepper;
   int pad_stepper;
+  // mixed form: FP32 copies of the constants its stepping loop reads, and the
+  // FP64 band -- an attempt that starts at r < band_r, or with theta within
+  // pole_band of a pole, is handed to the FP64 pass
+  float mass_f, spin_f, rs_f, atol_f, rtol_f;
+  float max_radius_hi, max_radius_lo;  // max_radius as an unevaluated float pair
+  float band_r, pole_band;
+  float pad_mixed;
   // sampling
   uint32_t width, height, spa, spp, jitter_spp, sub_w, sub_h;
   uint32_t pad0;
@@ -74,6 +81,19 @@ struct DevOutputs {
   double* cross;
   uint8_t* rgb8;        // image, written directly when spp == 1
   double* sample_rgb;   // 3*n linear sample colours, reduced per pixel when spp > 1
+  struct QueuedRay* queue;  // mixed form: rays handed to the FP64 pass
+  uint64_t queue_cap;
+};
+
+// A ray the mixed-precision pass hands to the FP64 pass: its state at the
+// start of the attempt that entered the FP64 band, in FP64.
+struct QueuedRay {
+  double x[4];
+  double v[4];
+  double h;
+  double lam;
+  uint64_t idx;  // sample index
+  uint32_t n_att, n_acc;
 };
 
 // Device-side counters of one render (reset before each launch).
@@ -84,7 +104,10 @@ struct DevControl {
   unsigned long long class_count[5];
   unsigned long long budget_used;
   unsigned int abort;            // set once the attempt budget is spent
-  unsigned int pad;
+  unsigned int queue_overflow;   // a mixed-form hand-off found the queue full
+  unsigned long long queued;     // rays handed to the FP64 pass
+  unsigned long long next_queued;  // the FP64 pass's queue head
+  unsigned long long fp64_attempts;  // attempts made in the FP64 pass
 };
 
 }  // namespace gg

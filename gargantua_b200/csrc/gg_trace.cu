@@ -16,122 +16,24 @@
 
 #include "gg_device.cuh"
 #include "gg_launch.h"
+#include "gg_trace_common.cuh"
 
 namespace gg {
 
 namespace {
 
-constexpr unsigned kFull = 0xffffffffu;
-#ifndef GG_TRACE_PERIOD
-#define GG_TRACE_PERIOD 4
-#endif
-constexpr int kPeriod = GG_TRACE_PERIOD;  // attempts between refills
-constexpr uint32_t kChunk = 32;  // samples a warp takes from the queue at once
-
-GG_DEV unsigned lanemask_lt() {
-  unsigned m;
-  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
-  return m;
-}
-
-// Writes the finished sample's outcome and colour.  Runs once per ray, so it
-// is kept out of line: its shading code (several pow) would otherwise sit in
-// the hot stepping loop's instruction footprint.
-__device__ __noinline__ void finish_sample(const DevParams& P, const DevOutputs& O, uint64_t idx,
-                                           int cls, Ray R, uint32_t n_att, uint32_t n_acc,
-                                           double intensity, double color_temp, bool crossed) {
-  {
-    const uint64_t n = P.n_rays;
-    double lin[3];
-    if (cls == kClsHorizon || cls == kClsBudget) {
-      lin[0] = lin[1] = lin[2] = 0.0;
-    } else if (cls == kClsEscaped) {
-      if (P.sky == kSkyChecker)
-        checker_sky(P, R.x[2], R.x[3], lin);
-      else
-        procedural_sky(R.v, lin);
-    } else if (cls == kClsDisk) {
-      disk_color(intensity, lin);
-    } else {
-      lin[0] = 0.0;
-      lin[1] = 0.0;
-      lin[2] = 10.0 / 255.0;
-    }
-    if (O.cls) O.cls[idx] = cls;
-    if (O.x) {
-#pragma unroll
-      for (int c = 0; c < 4; ++c) O.x[c * n + idx] = R.x[c];
-    }
-    if (O.v) {
-#pragma unroll
-      for (int c = 0; c < 4; ++c) O.v[c * n + idx] = R.v[c];
-    }
-    if (O.lam) O.lam[idx] = R.lam;
-    if (O.attempts) O.attempts[idx] = n_att;
-    if (O.accepted) O.accepted[idx] = n_acc;
-    if (O.intensity) O.intensity[idx] = intensity;
-    if (O.color_temp) O.color_temp[idx] = color_temp;
-    if (O.rgb) {
-#pragma unroll
-      for (int c = 0; c < 3; ++c) O.rgb[3 * idx + c] = lin[c];
-    }
-    if (O.cross && !crossed) {
-      const double qnan = __longlong_as_double(0x7ff8000000000000LL);
-#pragma unroll
-      for (int c = 0; c < 8; ++c) O.cross[c * n + idx] = qnan;
-    }
-    if (O.sample_rgb) {
-#pragma unroll
-      for (int c = 0; c < 3; ++c) O.sample_rgb[3 * idx + c] = lin[c];
-    } else if (O.rgb8) {
-#pragma unroll
-      for (int c = 0; c < 3; ++c) O.rgb8[3 * idx + c] = encode_channel(lin[c]);
-    }
-  }
-}
-
-// Camera ray of sample idx (once per ray, out of line like finish_sample).
-__device__ __noinline__ Ray start_sample(const DevParams& P, uint64_t idx) {
-  double u, v;
-  sample_uv(P, idx, u, v);
-  Ray R;
-  init_ray(P, u, v, R);
-  return R;
-}
-
-// Per-block totals of the statistics (one shared-memory atomic per finished
-// ray instead of per-thread counters, which would cost registers in the
-// stepping loop); flushed to DevControl when the block exits.
-struct BlockStats {
-  unsigned long long attempts, accepted, cls[5];
-};
-
-// Point at fraction s of the last accepted Euler segment (the reference moves
-// x by h*v_before, geodesic.rs:312, so x is linear in s); v interpolated.
-GG_DEV void segment_point(const double xb[4], const double vb[4], double h, const double va[4],
-                          double s, double out[8]) {
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const double raw = xb[i] + h * vb[i];
-    out[i] = xb[i] + s * (raw - xb[i]);
-    out[4 + i] = vb[i] + s * (va[i] - vb[i]);
-  }
-  normalize_coords(out);
-}
-
-GG_DEV void store_cross(const DevParams& P, const DevOutputs& O, uint64_t idx,
-                        const double c[8]) {
-  if (!O.cross) return;
-#pragma unroll
-  for (int i = 0; i < 8; ++i) O.cross[i * P.n_rays + idx] = c[i];
-}
-
-template <int METRIC, int DISK, int STEPPER>
+// SRC: kSrcCamera traces the render's samples from the camera; kSrcQueue
+// finishes, in FP64, the rays the mixed-precision pass handed over (their
+// count is read from ctl->queued, which that pass wrote before this launch).
+template <int METRIC, int DISK, int STEPPER, int SRC>
 __global__ void __launch_bounds__(kTraceBlock,
                                   METRIC == kMetricKerr ? kTraceMinBlocksKerr : kTraceMinBlocksSchw)
     trace_fp64_kernel(const __grid_constant__ DevParams P, const __grid_constant__ DevOutputs O,
                       DevControl* ctl) {
   const unsigned lane = threadIdx.x & 31u;
+  const uint64_t n_src =
+      SRC == kSrcQueue ? (ctl->queued < O.queue_cap ? ctl->queued : O.queue_cap) : P.n_rays;
+  unsigned long long* const head = SRC == kSrcQueue ? &ctl->next_queued : &ctl->next_ray;
   __shared__ BlockStats bs;
   __shared__ double k_smem[7][4][kTraceBlock];  // stage derivatives, see KStore
   const KStore K{k_smem};
@@ -145,6 +47,7 @@ __global__ void __launch_bounds__(kTraceBlock,
     atomicAdd(&bs.accepted, (unsigned long long)nc);
     atomicAdd(&bs.cls[cls], 1ull);
   };
+  uint32_t n_att0 = 0;  // kSrcQueue: attempts the ray had made before the hand-off
 
   Ray R;
   uint64_t idx = 0;
@@ -172,33 +75,47 @@ __global__ void __launch_bounds__(kTraceBlock,
       if (wcount == 0) {
         unsigned long long b = 0;
         if (lane == 0) {
-          b = atomicAdd(&ctl->next_ray, (unsigned long long)kChunk);
+          b = atomicAdd(head, (unsigned long long)kChunk);
           if (P.attempt_budget) {
             const unsigned long long used = atomicAdd(&ctl->budget_used, 0ull);
             if (used > P.attempt_budget) {
               atomicExch(&ctl->abort, 1u);
-              b = P.n_rays;  // stop taking work
+              b = n_src;  // stop taking work
             }
           }
         }
         b = __shfl_sync(kFull, b, 0);
-        if (b >= P.n_rays) {
+        if (b >= n_src) {
           wdone = true;
           break;
         }
         wbase = b;
-        const uint64_t left = P.n_rays - b;
+        const uint64_t left = n_src - b;
         wcount = left < kChunk ? (uint32_t)left : kChunk;
       }
       const unsigned nn = (unsigned)__popc(need);
       const unsigned take = nn < wcount ? nn : wcount;
       const unsigned rank = (unsigned)__popc(need & lanemask_lt());
       if (!live && rank < take) {
-        idx = wbase + rank;
-        R = start_sample(P, idx);
+        if (SRC == kSrcQueue) {
+          const QueuedRay& q = O.queue[wbase + rank];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            R.x[i] = q.x[i];
+            R.v[i] = q.v[i];
+          }
+          R.h = q.h;
+          R.lam = q.lam;
+          idx = q.idx;
+          n_att = n_att0 = q.n_att;
+          n_acc = q.n_acc;
+        } else {
+          idx = wbase + rank;
+          R = start_sample(P, idx);
+          n_att = 0;
+          n_acc = 0;
+        }
         live = true;
-        n_att = 0;
-        n_acc = 0;
         inten = 0.0;
         trans = 1.0;
         crossed = false;
@@ -354,6 +271,7 @@ __global__ void __launch_bounds__(kTraceBlock,
       }
       if (done_cls >= 0) {
         finish(idx, done_cls, R, n_att, n_acc, out_int, out_temp, crossed);
+        if (SRC == kSrcQueue) atomicAdd(&bs.fp64_att, (unsigned long long)(n_att - n_att0));
         budget_pending += n_att;
         live = false;
       }
@@ -372,6 +290,7 @@ __global__ void __launch_bounds__(kTraceBlock,
         wdone = true;
         if (live) {
           finish(idx, kClsBudget, R, n_att, n_acc, 0.0, 0.0, crossed);
+          if (SRC == kSrcQueue) atomicAdd(&bs.fp64_att, (unsigned long long)(n_att - n_att0));
           live = false;
         }
       }
@@ -383,6 +302,7 @@ __global__ void __launch_bounds__(kTraceBlock,
   if (threadIdx.x == 0) {
     atomicAdd(&ctl->attempts, bs.attempts);
     atomicAdd(&ctl->accepted, bs.accepted);
+    if (SRC == kSrcQueue && bs.fp64_att) atomicAdd(&ctl->fp64_attempts, bs.fp64_att);
 #pragma unroll
     for (int k = 0; k < 5; ++k)
       if (bs.cls[k]) atomicAdd(&ctl->class_count[k], bs.cls[k]);
@@ -407,21 +327,23 @@ __global__ void reduce_samples_kernel(const __grid_constant__ DevParams P, const
   }
 }
 
-template <int METRIC, int DISK, int STEPPER>
+template <int METRIC, int DISK, int STEPPER, int SRC>
 const void* trace_fn() {
-  return reinterpret_cast<const void*>(&trace_fp64_kernel<METRIC, DISK, STEPPER>);
+  return reinterpret_cast<const void*>(&trace_fp64_kernel<METRIC, DISK, STEPPER, SRC>);
 }
 
 template <int STEPPER>
 const void* select_metric_disk(const DevParams& P) {
   if (P.metric == kMetricKerr) {
-    if (P.disk == kDiskThin) return trace_fn<kMetricKerr, kDiskThin, STEPPER>();
-    if (P.disk == kDiskVolumetric) return trace_fn<kMetricKerr, kDiskVolumetric, STEPPER>();
-    return trace_fn<kMetricKerr, kDiskNone, STEPPER>();
+    if (P.disk == kDiskThin) return trace_fn<kMetricKerr, kDiskThin, STEPPER, kSrcCamera>();
+    if (P.disk == kDiskVolumetric)
+      return trace_fn<kMetricKerr, kDiskVolumetric, STEPPER, kSrcCamera>();
+    return trace_fn<kMetricKerr, kDiskNone, STEPPER, kSrcCamera>();
   }
-  if (P.disk == kDiskThin) return trace_fn<kMetricSchwarzschild, kDiskThin, STEPPER>();
-  if (P.disk == kDiskVolumetric) return trace_fn<kMetricSchwarzschild, kDiskVolumetric, STEPPER>();
-  return trace_fn<kMetricSchwarzschild, kDiskNone, STEPPER>();
+  if (P.disk == kDiskThin) return trace_fn<kMetricSchwarzschild, kDiskThin, STEPPER, kSrcCamera>();
+  if (P.disk == kDiskVolumetric)
+    return trace_fn<kMetricSchwarzschild, kDiskVolumetric, STEPPER, kSrcCamera>();
+  return trace_fn<kMetricSchwarzschild, kDiskNone, STEPPER, kSrcCamera>();
 }
 
 const void* select_trace(const DevParams& P) {
@@ -429,11 +351,35 @@ const void* select_trace(const DevParams& P) {
                                    : select_metric_disk<kStepperReference>(P);
 }
 
+// The FP64 pass of the mixed form: full Dormand-Prince, thin disk or none.
+const void* select_queue_trace(const DevParams& P) {
+  if (P.metric == kMetricKerr)
+    return P.disk == kDiskThin ? trace_fn<kMetricKerr, kDiskThin, kStepperDP45, kSrcQueue>()
+                               : trace_fn<kMetricKerr, kDiskNone, kStepperDP45, kSrcQueue>();
+  return P.disk == kDiskThin
+             ? trace_fn<kMetricSchwarzschild, kDiskThin, kStepperDP45, kSrcQueue>()
+             : trace_fn<kMetricSchwarzschild, kDiskNone, kStepperDP45, kSrcQueue>();
+}
+
 }  // namespace
 
 cudaError_t trace_occupancy(const DevParams& P, int* blocks_per_sm) {
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, select_trace(P),
                                                        kTraceBlock, 0);
+}
+
+cudaError_t queue_trace_occupancy(const DevParams& P, int* blocks_per_sm) {
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, select_queue_trace(P),
+                                                       kTraceBlock, 0);
+}
+
+cudaError_t launch_queue_trace(const DevParams& P, const DevOutputs& O, DevControl* ctl,
+                               int grid, cudaStream_t stream) {
+  const void* fn = select_queue_trace(P);
+  DevParams p = P;
+  DevOutputs o = O;
+  void* args[] = {&p, &o, &ctl};
+  return cudaLaunchKernel(fn, dim3(grid), dim3(kTraceBlock), args, 0, stream);
 }
 
 cudaError_t launch_trace(const DevParams& P, const DevOutputs& O, DevControl* ctl, int grid,

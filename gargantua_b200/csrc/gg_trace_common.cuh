@@ -1,0 +1,127 @@
+// gg_trace_common.cuh -- lane bookkeeping shared by the persistent trace
+// kernels (the FP64 kernel in gg_trace.cu, the mixed-precision kernel in
+// gg_mixed.cu): work-queue constants, sample setup and finishing, per-block
+// statistics and the crossing-state output.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "gg_device.cuh"
+#include "gg_launch.h"
+
+namespace gg {
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+#ifndef GG_TRACE_PERIOD
+#define GG_TRACE_PERIOD 4
+#endif
+constexpr int kPeriod = GG_TRACE_PERIOD;  // attempts between refills
+constexpr uint32_t kChunk = 32;  // samples a warp takes from the queue at once
+
+GG_DEV unsigned lanemask_lt() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// Writes the finished sample's outcome and colour.  Runs once per ray, so it
+// is kept out of line: its shading code (several pow) would otherwise sit in
+// the hot stepping loop's instruction footprint.
+__device__ __noinline__ void finish_sample(const DevParams& P, const DevOutputs& O, uint64_t idx,
+                                           int cls, Ray R, uint32_t n_att, uint32_t n_acc,
+                                           double intensity, double color_temp, bool crossed) {
+  {
+    const uint64_t n = P.n_rays;
+    double lin[3];
+    if (cls == kClsHorizon || cls == kClsBudget) {
+      lin[0] = lin[1] = lin[2] = 0.0;
+    } else if (cls == kClsEscaped) {
+      if (P.sky == kSkyChecker)
+        checker_sky(P, R.x[2], R.x[3], lin);
+      else
+        procedural_sky(R.v, lin);
+    } else if (cls == kClsDisk) {
+      disk_color(intensity, lin);
+    } else {
+      lin[0] = 0.0;
+      lin[1] = 0.0;
+      lin[2] = 10.0 / 255.0;
+    }
+    if (O.cls) O.cls[idx] = cls;
+    if (O.x) {
+#pragma unroll
+      for (int c = 0; c < 4; ++c) O.x[c * n + idx] = R.x[c];
+    }
+    if (O.v) {
+#pragma unroll
+      for (int c = 0; c < 4; ++c) O.v[c * n + idx] = R.v[c];
+    }
+    if (O.lam) O.lam[idx] = R.lam;
+    if (O.attempts) O.attempts[idx] = n_att;
+    if (O.accepted) O.accepted[idx] = n_acc;
+    if (O.intensity) O.intensity[idx] = intensity;
+    if (O.color_temp) O.color_temp[idx] = color_temp;
+    if (O.rgb) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) O.rgb[3 * idx + c] = lin[c];
+    }
+    if (O.cross && !crossed) {
+      const double qnan = __longlong_as_double(0x7ff8000000000000LL);
+#pragma unroll
+      for (int c = 0; c < 8; ++c) O.cross[c * n + idx] = qnan;
+    }
+    if (O.sample_rgb) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) O.sample_rgb[3 * idx + c] = lin[c];
+    } else if (O.rgb8) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) O.rgb8[3 * idx + c] = encode_channel(lin[c]);
+    }
+  }
+}
+
+// Camera ray of sample idx (once per ray, out of line like finish_sample).
+__device__ __noinline__ Ray start_sample(const DevParams& P, uint64_t idx) {
+  double u, v;
+  sample_uv(P, idx, u, v);
+  Ray R;
+  init_ray(P, u, v, R);
+  return R;
+}
+
+// Per-block totals of the statistics (one shared-memory atomic per finished
+// ray instead of per-thread counters, which would cost registers in the
+// stepping loop); flushed to DevControl when the block exits.
+struct BlockStats {
+  unsigned long long attempts, accepted, cls[5], fp64_att;
+};
+
+enum : int { kSrcCamera = 0, kSrcQueue = 1 };
+
+// Point at fraction s of the last accepted Euler segment (the reference moves
+// x by h*v_before, geodesic.rs:312, so x is linear in s); v interpolated.
+GG_DEV void segment_point(const double xb[4], const double vb[4], double h, const double va[4],
+                          double s, double out[8]) {
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const double raw = xb[i] + h * vb[i];
+    out[i] = xb[i] + s * (raw - xb[i]);
+    out[4 + i] = vb[i] + s * (va[i] - vb[i]);
+  }
+  normalize_coords(out);
+}
+
+GG_DEV void store_cross(const DevParams& P, const DevOutputs& O, uint64_t idx,
+                        const double c[8]) {
+  if (!O.cross) return;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) O.cross[i * P.n_rays + idx] = c[i];
+}
+
+}  // namespace
+
+}  // namespace gg

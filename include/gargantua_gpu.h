@@ -162,7 +162,11 @@ typedef struct gg_stats_t {
   uint64_t attempts;
   uint64_t accepted;
   uint64_t class_count[5];
-  double kernel_ms; /* device time of the trace launch                      */
+  double kernel_ms; /* device time of the trace launch(es)                 */
+  /* GG_PREC_MIXED: rays the FP32 pass handed to the FP64 pass (FP64 band)
+   * and the attempts made in that pass; 0 for GG_PREC_FP64 */
+  uint64_t fp64_rays;
+  uint64_t fp64_attempts;
 } gg_stats_t;
 
 typedef struct gg_ctx gg_ctx;
