@@ -129,6 +129,7 @@ _SIGNATURES = {
                                    P(gg_integrator_t), P(gg_render_opts_t), C.c_uint32,
                                    C.c_uint32, C.c_void_p, P(gg_ray_out_t), C.c_void_p]),
     "gg_measure_fma_peak": (C.c_int, [C.c_void_p, C.c_int, P(C.c_double)]),
+    "gg_polar_sincos": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32]),
     "gg_render_device_noalloc": (C.c_int, [P(gg_metric_t), P(gg_camera_t), P(gg_disk_t),
                                            P(gg_integrator_t), P(gg_render_opts_t), C.c_uint32,
                                            C.c_uint32, C.c_void_p, P(gg_ray_out_t),

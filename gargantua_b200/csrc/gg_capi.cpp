@@ -40,6 +40,12 @@ struct gg_ctx {
   std::mutex mu;
 };
 
+// Half-width (rad) of the polar caps whose attempts the mixed form runs in
+// FP64 (tuning builds override it).
+#ifndef GG_POLE_BAND
+#define GG_POLE_BAND 0.1f
+#endif
+
 namespace {
 
 constexpr double kPi = 3.14159265358979323846;
@@ -225,7 +231,7 @@ void build_params(const gg_metric_t* metric, const gg_camera_t* camera, const gg
   // test radius (the photon orbit lies outside the horizon), and 0.1 rad of
   // the poles
   P.band_r = (float)(std::fmax(P.r_photon, P.rh_plus_buffer) + 0.5);
-  P.pole_band = 0.1f;
+  P.pole_band = GG_POLE_BAND;
 
   P.width = width;
   P.height = height;

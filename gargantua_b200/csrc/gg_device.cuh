@@ -552,6 +552,8 @@ struct DPTable {
   double A[7];        // stage node a_s (row sums of B)
   double E[7];        // c - d, velocity error weights
   double Ebar[7];     // position error weights of h^2 k_l
+  double D[7];        // continuous extension weights d_j (sum to zero)
+  double Dbar[7];     // their position form: sum_j d_j (w_j - v) = h sum_l Dbar_l k_l
 };
 
 constexpr DPTable make_dp_table() {
@@ -585,6 +587,17 @@ constexpr DPTable make_dp_table() {
     double eb = 0.0;
     for (int j = l + 1; j < 7; ++j) eb += (b[6][j] - d[j]) * b[j][l];
     t.Ebar[l] = eb;
+  }
+  // continuous extension of the pair (Shampine 1986; Hairer, Norsett &
+  // Wanner, Solving ODEs I, sec. II.6)
+  const double dd[7] = {-12715105075.0 / 11282082432.0, 0.0, 87487479700.0 / 32700410799.0,
+                        -10690763975.0 / 1880347072.0, 701980252875.0 / 199316789632.0,
+                        -1453857185.0 / 822651844.0, 69997945.0 / 29380423.0};
+  for (int l = 0; l < 7; ++l) {
+    t.D[l] = dd[l];
+    double db = 0.0;
+    for (int j = l + 1; j < 7; ++j) db += dd[j] * b[j][l];
+    t.Dbar[l] = db;
   }
   return t;
 }
@@ -711,43 +724,74 @@ GG_DEV int attempt_dp45_fp64(const DevParams& P, Ray& R, const KStore& K, bool& 
   return kContinue;
 }
 
-// Cubic Hermite interpolant of an accepted full Dormand-Prince step at
-// fraction s: positions from (x, v) at both ends, velocities from (v, a).
-GG_DEV void hermite_point(const double xb[4], const double vb[4], const double kb[4],
-                          const double xa[4], const double va[4], const double ka[4], double h,
-                          double s, double out[8]) {
-  const double s2 = s * s, s3 = s2 * s;
-  const double h00 = 2.0 * s3 - 3.0 * s2 + 1.0, h10 = s3 - 2.0 * s2 + s;
-  const double h01 = -2.0 * s3 + 3.0 * s2, h11 = s3 - s2;
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    out[i] = h00 * xb[i] + h10 * h * vb[i] + h01 * xa[i] + h11 * h * va[i];
-    out[4 + i] = h00 * vb[i] + h10 * h * kb[i] + h01 * va[i] + h11 * h * ka[i];
+// An accepted full Dormand-Prince step, for locating a crossing inside it:
+// start state, end state before angle normalisation, step, and the seven
+// stage accelerations k_1..k_7 (k_7 = a at the end).  Kernels fill one only
+// on the (once per ray) path where a crossing was detected.
+struct StepSpan {
+  double xb[4], vb[4], xa[4], va[4];
+  double k[7][4];
+  double h;
+};
+
+// Continuous extension of the Dormand-Prince pair (Shampine 1986; Hairer,
+// Norsett & Wanner, Solving ODEs I, sec. II.6), a 4th-order polynomial in the
+// step fraction s for each of the 8 components of y = (x, v):
+// y(s) = y0 + s (r2 + (1-s) (r3 + s (r4 + (1-s) r5))), r2 = y1 - y0,
+// r3 = h y'(0) - r2, r4 = r2 - h y'(1) - r3, r5 = h sum_j d_j F_j.  The d_j
+// sum to zero, so the position part of r5 is h^2 sum_l Dbar_l k_l.
+struct DenseComp {
+  double y0, r2, r3, r4, r5;
+  GG_DEV double at(double s) const {
+    const double t = 1.0 - s;
+    return y0 + s * (r2 + t * (r3 + s * (r4 + t * r5)));
   }
+  GG_DEV double slope(double s) const {
+    const double t = 1.0 - s;
+    return r2 + (1.0 - 2.0 * s) * r3 + s * (2.0 - 3.0 * s) * r4 + 2.0 * s * t * (1.0 - 2.0 * s) * r5;
+  }
+};
+
+GG_DEV DenseComp dense_comp(const StepSpan& sp, int c) {
+  DenseComp q;
+  double w = 0.0;
+  if (c < 4) {
+    for (int l = 0; l < 6; ++l) w = fma(kDP.Dbar[l], sp.k[l][c], w);
+    q.y0 = sp.xb[c];
+    q.r2 = sp.xa[c] - sp.xb[c];
+    q.r3 = sp.h * sp.vb[c] - q.r2;
+    q.r4 = q.r2 - sp.h * sp.va[c] - q.r3;
+    q.r5 = sp.h * sp.h * w;
+  } else {
+    const int i = c - 4;
+    for (int l = 0; l < 7; ++l) w = fma(kDP.D[l], sp.k[l][i], w);
+    q.y0 = sp.vb[i];
+    q.r2 = sp.va[i] - sp.vb[i];
+    q.r3 = sp.h * sp.k[0][i] - q.r2;
+    q.r4 = q.r2 - sp.h * sp.k[6][i] - q.r3;
+    q.r5 = sp.h * w;
+  }
+  return q;
 }
 
-// Fraction s where component c of the Hermite position meets `target`
-// (bracketed by the step's ends): safeguarded Newton, at most 30 steps.
-GG_DEV double hermite_root(const double xb[4], const double vb[4], const double xa[4],
-                           const double va[4], double h, int c, double target) {
-  const double p0 = xb[c], m0 = h * vb[c], p1 = xa[c], m1 = h * va[c];
-  auto f = [&](double s, double& df) {
-    const double s2 = s * s, s3 = s2 * s;
-    df = (6.0 * s2 - 6.0 * s) * p0 + (3.0 * s2 - 4.0 * s + 1.0) * m0 + (-6.0 * s2 + 6.0 * s) * p1 +
-         (3.0 * s2 - 2.0 * s) * m1;
-    return (2.0 * s3 - 3.0 * s2 + 1.0) * p0 + (s3 - 2.0 * s2 + s) * m0 +
-           (-2.0 * s3 + 3.0 * s2) * p1 + (s3 - s2) * m1 - target;
-  };
-  double lo = 0.0, hi = 1.0, d0, d1;
-  const double flo = f(0.0, d0);
-  const double fhi = f(1.0, d1);
+// Locates where component `comp` of the step's continuous extension meets
+// `target` (it changes sign across the step): safeguarded Newton from the
+// chord's root inside a shrinking bracket, at most 30 iterations.  Writes the
+// 8-component state there (angles not yet normalised) and returns the step
+// fraction.  Out of line: once per ray.
+static __device__ __noinline__ double dense_crossing(const StepSpan& sp, int comp, double target,
+                                              double out[8]) {
+  const DenseComp q = dense_comp(sp, comp);
+  const double flo = q.at(0.0) - target;
+  const double fhi = q.at(1.0) - target;
+  double lo = 0.0, hi = 1.0;
   double s = flo / (flo - fhi);
   if (!(s >= 0.0 && s <= 1.0)) s = 0.5;
   for (int it = 0; it < 30; ++it) {
-    double d;
-    const double fs = f(s, d);
+    const double fs = q.at(s) - target;
     if (fs == 0.0) break;
     if ((fs < 0.0) == (flo < 0.0)) lo = s; else hi = s;
+    const double d = q.slope(s);
     double sn = d != 0.0 ? s - fs / d : 0.5 * (lo + hi);
     if (!(sn > lo && sn < hi)) sn = 0.5 * (lo + hi);
     if (fabs(sn - s) <= 1e-15) {
@@ -756,6 +800,7 @@ GG_DEV double hermite_root(const double xb[4], const double vb[4], const double 
     }
     s = sn;
   }
+  for (int c = 0; c < 8; ++c) out[c] = dense_comp(sp, c).at(s);
   return s;
 }
 

@@ -14,12 +14,13 @@
 // back to back for lanes in different bands.
 //
 // Crossings of the escape sphere and the disk plane are detected on the
-// float-pair differences and located in FP64 on the step's cubic Hermite
-// interpolant, as in the FP64 kernel.
+// float-pair differences and located in FP64 on the step's continuous
+// extension (the Dormand-Prince dense output), as in the FP64 kernel.
 #include <cuda_runtime.h>
 
 #include <cstdint>
 
+#include "../../include/gargantua_gpu.h"
 #include "gg_device.cuh"
 #include "gg_launch.h"
 #include "gg_mixed.cuh"
@@ -58,7 +59,8 @@ __device__ __noinline__ void hand_off(const DevOutputs& O, DevControl* ctl, Mixe
 __device__ __noinline__ void mixed_finish(const DevParams& P, const DevOutputs& O, MixedSmem K,
                                           MixedRegs S, int cls, uint32_t n_att, uint32_t n_acc,
                                           bool crossed, BlockStats* bs) {
-  finish_sample(P, O, K.idx(), cls, mixed_fp64(K, S), n_att, n_acc, 0.0, 0.0, crossed);
+  const Ray R = mixed_fp64(K, S);
+  finish_sample(P, O, K.idx(), cls, R, n_att, n_acc, 0.0, 0.0, crossed, R.x[2], R.x[3]);
   atomicAdd(&bs->attempts, (unsigned long long)n_att);
   atomicAdd(&bs->accepted, (unsigned long long)n_acc);
   atomicAdd(&bs->cls[cls], 1ull);
@@ -66,38 +68,51 @@ __device__ __noinline__ void mixed_finish(const DevParams& P, const DevOutputs& 
 
 // The accepted step (pre-step state, increments in slots 7, 8, k1 in slot
 // 0, k7 in slot 6) crossed the escape sphere (`esc`) and/or the disk
-// plane (`dsk`): locate the crossings in FP64 on the Hermite interpolant.
-// Stores the escape crossing; when the ray ends on the thin disk, writes its
-// outcome at the crossing and returns true.
+// plane (`dsk`): locate the crossings in FP64 on the step's continuous
+// extension.
+// Stores the escape crossing.  When the ray ends here -- on the thin disk,
+// or, with the checkerboard sky, at the escape sphere (whose cell is read at
+// the crossing; the next attempt would only find r > max_radius and return
+// Escaped, and is counted) -- writes its outcome and returns the attempts it
+// ended with, else 0.
 template <int METRIC, int DISK>
-__device__ __noinline__ bool mixed_crossings(const DevParams& P, const DevOutputs& O, MixedSmem K,
+__device__ __noinline__ uint32_t mixed_crossings(const DevParams& P, const DevOutputs& O, MixedSmem K,
                                              MixedRegs S, float hf, bool esc, bool dsk,
                                              uint32_t n_att, uint32_t n_acc, BlockStats* bs) {
   const Ray B = mixed_fp64(K, S);
   const uint64_t idx = K.idx();
-  const float4 dx4 = K.get(kSlotDx), dv4 = K.get(kSlotDv), k14 = K.get(0), k74 = K.get(6);
+  const float4 dx4 = K.get(kSlotDx), dv4 = K.get(kSlotDv);
   const float dx[4] = {dx4.x, dx4.y, dx4.z, dx4.w}, dv[4] = {dv4.x, dv4.y, dv4.z, dv4.w};
-  const float k1[4] = {k14.x, k14.y, k14.z, k14.w}, k7[4] = {k74.x, k74.y, k74.z, k74.w};
-  double xa[4], va[4], kb[4], ka[4];
+  StepSpan sp;
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
-    xa[i] = B.x[i] + (double)dx[i];
-    va[i] = B.v[i] + (double)dv[i];
-    kb[i] = (double)k1[i];
-    ka[i] = (double)k7[i];
+    sp.xb[i] = B.x[i];
+    sp.vb[i] = B.v[i];
+    sp.xa[i] = B.x[i] + (double)dx[i];
+    sp.va[i] = B.v[i] + (double)dv[i];
   }
-  const double h = (double)hf;
-  if (esc && O.cross) {
-    const double s = hermite_root(B.x, B.v, xa, va, h, 1, P.max_radius);
+  for (int l = 0; l < 7; ++l) {
+    const float4 k = K.get(l);
+    sp.k[l][0] = k.x;
+    sp.k[l][1] = k.y;
+    sp.k[l][2] = k.z;
+    sp.k[l][3] = k.w;
+  }
+  sp.h = (double)hf;
+  bool esc_end = false;
+  double sky_th = 0.0, sky_ph = 0.0;
+  if (esc && (O.cross || P.sky == kSkyChecker)) {
     double c[8];
-    hermite_point(B.x, B.v, kb, xa, va, ka, h, s, c);
+    dense_crossing(sp, 1, P.max_radius, c);
     normalize_coords(c);
-    store_cross(P, O, idx, c);
+    if (O.cross) store_cross(P, O, idx, c);
+    esc_end = P.sky == kSkyChecker;
+    sky_th = c[2];
+    sky_ph = c[3];
   }
   if (DISK == kDiskThin && dsk) {
-    const double s = hermite_root(B.x, B.v, xa, va, h, 2, kHalfPi);
     double c[8];
-    hermite_point(B.x, B.v, kb, xa, va, ka, h, s, c);
+    const double s = dense_crossing(sp, 2, kHalfPi, c);
     normalize_coords(c);
     const double r_c = c[1];
     if (r_c >= P.r_inner && r_c <= P.r_outer) {
@@ -112,17 +127,34 @@ __device__ __noinline__ bool mixed_crossings(const DevParams& P, const DevOutput
         end.v[i] = c[4 + i];
       }
       end.h = S.h;
-      end.lam = B.lam + s * h;
+      end.lam = B.lam + s * sp.h;
       store_cross(P, O, idx, c);
       finish_sample(P, O, idx, kClsDisk, end, n_att, n_acc, (g2 * g2) * pow(q, P.emissivity_index),
-                    g * pow(q, 0.75), true);
+                    g * pow(q, 0.75), true, c[2], c[3]);
       atomicAdd(&bs->attempts, (unsigned long long)n_att);
       atomicAdd(&bs->accepted, (unsigned long long)n_acc);
       atomicAdd(&bs->cls[kClsDisk], 1ull);
-      return true;
+      return n_att;
     }
   }
-  return false;
+  if (esc_end && n_att < P.max_steps) {
+    Ray end;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      end.x[i] = sp.xa[i];
+      end.v[i] = sp.va[i];
+    }
+    normalize_coords(end.x);
+    end.h = S.h;
+    end.lam = B.lam + sp.h;
+    const uint32_t na = n_att + 1;
+    finish_sample(P, O, idx, kClsEscaped, end, na, n_acc, 0.0, 0.0, true, sky_th, sky_ph);
+    atomicAdd(&bs->attempts, (unsigned long long)na);
+    atomicAdd(&bs->accepted, (unsigned long long)n_acc);
+    atomicAdd(&bs->cls[kClsEscaped], 1ull);
+    return na;
+  }
+  return 0;
 }
 
 // BUDGET: the render has an attempt budget (its bookkeeping costs registers,
@@ -241,8 +273,10 @@ __global__ void __launch_bounds__(kTraceBlock, kMixedMinBlocks)
         }
         if (esc || dsk) {
           if (esc && O.cross) crossed = true;
-          if (mixed_crossings<METRIC, DISK>(P, O, K, S, hf, esc, dsk, n_att, n_acc, &bs)) {
-            if (BUDGET) budget_pending += n_att;
+          const uint32_t ended =
+              mixed_crossings<METRIC, DISK>(P, O, K, S, hf, esc, dsk, n_att, n_acc, &bs);
+          if (ended) {
+            if (BUDGET) budget_pending += ended;
             live = false;
             continue;
           }
@@ -324,9 +358,7 @@ cudaError_t launch_mixed(const DevParams& P, const DevOutputs& O, DevControl* ct
 
 // The mixed kernel's polar-angle sincos evaluated on the host from the same
 // source, so tests can check it against a double-precision reference.
-extern "C" __attribute__((visibility("default"))) int gg_polar_sincos(const float* theta,
-                                                                       float* s, float* c,
-                                                                       uint32_t n) {
+extern "C" GG_API int gg_polar_sincos(const float* theta, float* s, float* c, uint32_t n) {
   if (!theta || !s || !c) return -1;
   for (uint32_t i = 0; i < n; ++i) gg::sincos_polar(theta[i], s + i, c + i);
   return 0;

@@ -41,8 +41,8 @@ __global__ void __launch_bounds__(kTraceBlock,
     reinterpret_cast<unsigned long long*>(&bs)[threadIdx.x] = 0ull;
   __syncthreads();
   auto finish = [&](uint64_t i, int cls, const Ray& r, uint32_t na, uint32_t nc, double inten_o,
-                    double temp_o, bool cr) {
-    finish_sample(P, O, i, cls, r, na, nc, inten_o, temp_o, cr);
+                    double temp_o, bool cr, double sky_th, double sky_ph) {
+    finish_sample(P, O, i, cls, r, na, nc, inten_o, temp_o, cr, sky_th, sky_ph);
     atomicAdd(&bs.attempts, (unsigned long long)na);
     atomicAdd(&bs.accepted, (unsigned long long)nc);
     atomicAdd(&bs.cls[cls], 1ull);
@@ -151,46 +151,71 @@ __global__ void __launch_bounds__(kTraceBlock,
       if (acc) n_acc += 1;
       int done_cls = -1;
       double out_int = 0.0, out_temp = 0.0;
+      // full Dormand-Prince, checkerboard sky, thin disk or none: the sky is
+      // read where the ray meets the escape sphere (sky_at_cross)
+      constexpr bool kSkyCross = STEPPER == kStepperDP45 && DISK != kDiskVolumetric;
+      bool sky_at_cross = false;
+      double sky_th = 0.0, sky_ph = 0.0;
 
       if (acc) {
         // The step's path: the reference's Euler segment (exactly linear in
-        // the step fraction), or the full Dormand-Prince step's cubic Hermite.
+        // the step fraction), or the full Dormand-Prince step's continuous
+        // extension.
         double raw[4];
 #pragma unroll
         for (int i = 0; i < 4; ++i)
           raw[i] = STEPPER == kStepperDP45 ? end.xraw[i] : xb[i] + h_used * vb[i];
-        auto point = [&](double s, double c[8]) {
+        const bool esc = (O.cross || (kSkyCross && P.sky == kSkyChecker)) &&
+                         xb[1] <= P.max_radius && raw[1] > P.max_radius;
+        double d_b = 0.0, d_a = 0.0;
+        bool dsk = false;
+        if (DISK == kDiskThin) {
+          d_b = xb[2] - kHalfPi;
+          d_a = R.x[2] - kHalfPi;
+          dsk = (d_b < 0.0 && d_a >= 0.0) || (d_b > 0.0 && d_a <= 0.0);
+        }
+        if (esc || dsk) {
+          StepSpan sp;
           if (STEPPER == kStepperDP45) {
-            double ka[4], kb[4];
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
-              kb[i] = K(0, i);
-              ka[i] = K(6, i);
+              sp.xb[i] = xb[i];
+              sp.vb[i] = vb[i];
+              sp.xa[i] = raw[i];
+              sp.va[i] = R.v[i];
             }
-            hermite_point(xb, vb, kb, raw, R.v, ka, h_used, s, c);
-            normalize_coords(c);
-          } else {
-            segment_point(xb, vb, h_used, R.v, s, c);
+            for (int l = 0; l < 7; ++l)
+#pragma unroll
+              for (int i = 0; i < 4; ++i) sp.k[l][i] = K(l, i);
+            sp.h = h_used;
           }
-        };
-        auto root = [&](int comp, double target, double linear_s) {
-          return STEPPER == kStepperDP45 ? hermite_root(xb, vb, raw, R.v, h_used, comp, target)
-                                         : linear_s;
-        };
-        // escape-sphere crossing on this step
-        if (O.cross && xb[1] <= P.max_radius && raw[1] > P.max_radius) {
-          double c[8];
-          point(root(1, P.max_radius, (P.max_radius - xb[1]) / (raw[1] - xb[1])), c);
-          store_cross(P, O, idx, c);
-          crossed = true;
-        }
-        if (DISK == kDiskThin) {
-          const double d_b = xb[2] - kHalfPi;
-          const double d_a = R.x[2] - kHalfPi;
-          if ((d_b < 0.0 && d_a >= 0.0) || (d_b > 0.0 && d_a <= 0.0)) {
-            const double s = root(2, kHalfPi, d_b / (d_b - d_a));
+          // state c where component `comp` meets `target`; returns the step
+          // fraction (the reference stepper's is linear_s, on its segment)
+          auto cross_at = [&](int comp, double target, double linear_s, double c[8]) {
+            if (STEPPER == kStepperDP45) {
+              const double s = dense_crossing(sp, comp, target, c);
+              normalize_coords(c);
+              return s;
+            }
+            segment_point(xb, vb, h_used, R.v, linear_s, c);
+            return linear_s;
+          };
+          if (esc) {
             double c[8];
-            point(s, c);
+            cross_at(1, P.max_radius, (P.max_radius - xb[1]) / (raw[1] - xb[1]), c);
+            if (O.cross) {
+              store_cross(P, O, idx, c);
+              crossed = true;
+            }
+            if (kSkyCross && P.sky == kSkyChecker) {
+              sky_at_cross = true;
+              sky_th = c[2];
+              sky_ph = c[3];
+            }
+          }
+          if (dsk) {
+            double c[8];
+            const double s = cross_at(2, kHalfPi, d_b / (d_b - d_a), c);
             const double r_c =
                 STEPPER == kStepperDP45 ? c[1] : xb[1] + s * (raw[1] - xb[1]);
             if (r_c >= P.r_inner && r_c <= P.r_outer) {
@@ -212,6 +237,12 @@ __global__ void __launch_bounds__(kTraceBlock,
               done_cls = kClsDisk;
             }
           }
+        }
+        // Beyond the escape sphere the next attempt only finds r > max_radius
+        // and returns Escaped; the ray ends here, counting that attempt.
+        if (sky_at_cross && done_cls < 0 && n_att < P.max_steps) {
+          n_att += 1;
+          done_cls = kClsEscaped;
         }
       }
       if (DISK == kDiskVolumetric && done_cls < 0) {
@@ -270,7 +301,8 @@ __global__ void __launch_bounds__(kTraceBlock,
         else if (n_att >= P.max_steps) done_cls = kClsMaxSteps;
       }
       if (done_cls >= 0) {
-        finish(idx, done_cls, R, n_att, n_acc, out_int, out_temp, crossed);
+        finish(idx, done_cls, R, n_att, n_acc, out_int, out_temp, crossed,
+               sky_at_cross ? sky_th : R.x[2], sky_at_cross ? sky_ph : R.x[3]);
         if (SRC == kSrcQueue) atomicAdd(&bs.fp64_att, (unsigned long long)(n_att - n_att0));
         budget_pending += n_att;
         live = false;
@@ -289,7 +321,7 @@ __global__ void __launch_bounds__(kTraceBlock,
       if (__shfl_sync(kFull, ab, 0)) {
         wdone = true;
         if (live) {
-          finish(idx, kClsBudget, R, n_att, n_acc, 0.0, 0.0, crossed);
+          finish(idx, kClsBudget, R, n_att, n_acc, 0.0, 0.0, crossed, R.x[2], R.x[3]);
           if (SRC == kSrcQueue) atomicAdd(&bs.fp64_att, (unsigned long long)(n_att - n_att0));
           live = false;
         }

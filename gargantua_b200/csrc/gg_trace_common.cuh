@@ -30,10 +30,13 @@ GG_DEV unsigned lanemask_lt() {
 
 // Writes the finished sample's outcome and colour.  Runs once per ray, so it
 // is kept out of line: its shading code (several pow) would otherwise sit in
-// the hot stepping loop's instruction footprint.
+// the hot stepping loop's instruction footprint.  (sky_th, sky_ph) is where
+// the checkerboard sky is read: the final position, or, for the full
+// Dormand-Prince stepper, the escape-sphere crossing.
 __device__ __noinline__ void finish_sample(const DevParams& P, const DevOutputs& O, uint64_t idx,
                                            int cls, Ray R, uint32_t n_att, uint32_t n_acc,
-                                           double intensity, double color_temp, bool crossed) {
+                                           double intensity, double color_temp, bool crossed,
+                                           double sky_th, double sky_ph) {
   {
     const uint64_t n = P.n_rays;
     double lin[3];
@@ -41,7 +44,7 @@ __device__ __noinline__ void finish_sample(const DevParams& P, const DevOutputs&
       lin[0] = lin[1] = lin[2] = 0.0;
     } else if (cls == kClsEscaped) {
       if (P.sky == kSkyChecker)
-        checker_sky(P, R.x[2], R.x[3], lin);
+        checker_sky(P, sky_th, sky_ph, lin);
       else
         procedural_sky(R.v, lin);
     } else if (cls == kClsDisk) {

@@ -18,5 +18,17 @@ REFERENCE_ATTEMPT_FLOPS = {
 }
 
 
-def attempt_flops(metric_kind: str, rtol: float) -> int:
-    return REFERENCE_ATTEMPT_FLOPS[(metric_kind, "rtol" if rtol > 0.0 else "tol")]
+# The same count for one attempt of the full Dormand-Prince stepper
+# (abi.GG_STEPPER_DP45): the seven right-hand sides and the stage algebra
+# of all eight components, as the oracle's step_dp45 restates it.
+DP45_ATTEMPT_FLOPS = {
+    ("kerr", "rtol"): 3084,
+    ("kerr", "tol"): 3078,
+    ("schwarzschild", "rtol"): 956,
+    ("schwarzschild", "tol"): 950,
+}
+
+
+def attempt_flops(metric_kind: str, rtol: float, stepper: int = 0) -> int:
+    table = DP45_ATTEMPT_FLOPS if stepper == 1 else REFERENCE_ATTEMPT_FLOPS
+    return table[(metric_kind, "rtol" if rtol > 0.0 else "tol")]

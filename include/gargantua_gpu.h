@@ -94,7 +94,8 @@ typedef struct gg_disk_t {
  * position by h * vel (first order) and controls the velocity error only.
  * GG_STEPPER_DP45 is the full Dormand-Prince RK5(4) on (x, v): positions
  * from the stage velocities, error control over all eight components, the
- * reference's termination tests and step-size law, cubic Hermite crossings. */
+ * reference's termination tests and step-size law, crossings located on the
+ * pair's 4th-order continuous extension (dense output). */
 #define GG_STEPPER_REFERENCE 0
 #define GG_STEPPER_DP45 1
 
@@ -261,6 +262,11 @@ GG_API int gg_render_device_noalloc(const gg_metric_t* metric, const gg_camera_t
  * 0 for FP32.  The roofline denominator of the trace kernels.  No reference
  * counterpart (the reference has no device code). */
 GG_API int gg_measure_fma_peak(gg_ctx* ctx, int fp64, double* flops);
+/* sin and cos of n polar angles in FP32, by the routine the GG_PREC_MIXED
+ * kernel's right-hand side uses (theta in [-pi/4, 5 pi/4]), evaluated on the
+ * host from the same source so its accuracy can be checked without a GPU.
+ * 0, or -1 for a NULL pointer.  No reference counterpart. */
+GG_API int gg_polar_sincos(const float* theta, float* s, float* c, uint32_t n);
 
 #ifdef __cplusplus
 }

@@ -554,9 +554,10 @@ struct RK45 {
   int stepper = 0;
 
   // One attempt.  `accepted` (optional) reports whether the state advanced.
-  // k_ends (optional, 12 doubles) receives a(x, v) at the start and the end
-  // of an accepted full Dormand-Prince step and its un-normalised end
-  // position, for the crossing interpolant.
+  // k_ends (optional, 32 doubles) receives, for an accepted full
+  // Dormand-Prince step, its seven stage accelerations k_1..k_7 (4 each,
+  // k_7 = a at the new state) and its un-normalised end position, for the
+  // crossing interpolant (dense_build).
   template <class M, class T>
   StepResult step(const M& metric, State<T>& st, T& h, bool* accepted = nullptr,
                   T* h_used = nullptr, T* k_ends = nullptr) const {
@@ -720,11 +721,9 @@ struct RK45 {
     }
     if (err < tol || h <= T(min_step)) {
       if (k_ends) {
-        for (int i = 0; i < 4; ++i) {
-          k_ends[i] = k[0][i];
-          k_ends[4 + i] = k[6][i];
-          k_ends[8 + i] = xn[i];
-        }
+        for (int j = 0; j < 7; ++j)
+          for (int i = 0; i < 4; ++i) k_ends[4 * j + i] = k[j][i];
+        for (int i = 0; i < 4; ++i) k_ends[28 + i] = xn[i];
       }
       st.position = xn;
       st.velocity = vn;
@@ -740,46 +739,93 @@ struct RK45 {
   }
 };
 
-// EXTENSION: cubic Hermite interpolant of an accepted full Dormand-Prince
-// step at fraction s: position from (x, v) at both ends, velocity from (v, a).
-// xb/vb: start state; xa/va: end state before angle normalisation; ka/kb the
-// accelerations at start / end; out[8] = (x, v).
-inline void hermite_point(const double xb[4], const double vb[4], const double ka[4],
-                          const double xa[4], const double va[4], const double kb[4], double h,
-                          double s, double out[8]) {
-  const double s2 = s * s, s3 = s2 * s;
-  const double h00 = 2.0 * s3 - 3.0 * s2 + 1.0, h10 = s3 - 2.0 * s2 + s;
-  const double h01 = -2.0 * s3 + 3.0 * s2, h11 = s3 - s2;
+// EXTENSION: the continuous extension of the Dormand-Prince pair (Shampine
+// 1986; Hairer, Norsett & Wanner, Solving ODEs I, sec. II.6), a 4th-order
+// polynomial through an accepted step, used to locate and state the escape
+// sphere and disk plane crossings.  With y = (x, v), F_j = (w_j, k_j) the
+// stage derivatives (w_j stage velocities, k_j accelerations) and s in
+// [0, 1]:  y(s) = y0 + s (r2 + (1-s) (r3 + s (r4 + (1-s) r5))) with
+// r2 = y1 - y0, r3 = h F_1 - r2, r4 = r2 - h F_7 - r3, r5 = h sum_j d_j F_j.
+// The d_j sum to zero, so the position part of r5 is h sum_j d_j (w_j - v):
+// formed from the stage velocity increments, without cancellation.
+struct DenseStep {
+  double y0[8], r2[8], r3[8], r4[8], r5[8];
+};
+
+inline const double* dense_weights() {
+  static const double d[7] = {-12715105075.0 / 11282082432.0, 0.0,
+                              87487479700.0 / 32700410799.0, -10690763975.0 / 1880347072.0,
+                              701980252875.0 / 199316789632.0, -1453857185.0 / 822651844.0,
+                              69997945.0 / 29380423.0};
+  return d;
+}
+
+// xb, vb: start state; xa, va: end state before angle normalisation; k: the
+// step's k_1..k_7 (7 x 4); h: the step.
+inline void dense_build(const double xb[4], const double vb[4], const double xa[4],
+                        const double va[4], const double* k, double h, DenseStep& D) {
+  const double B[7][6] = {
+      {0, 0, 0, 0, 0, 0},
+      {1.0 / 5.0, 0, 0, 0, 0, 0},
+      {3.0 / 40.0, 9.0 / 40.0, 0, 0, 0, 0},
+      {44.0 / 45.0, -56.0 / 15.0, 32.0 / 9.0, 0, 0, 0},
+      {19372.0 / 6561.0, -25360.0 / 2187.0, 64448.0 / 6561.0, -212.0 / 729.0, 0, 0},
+      {9017.0 / 3168.0, -355.0 / 33.0, 46732.0 / 5247.0, 49.0 / 176.0, -5103.0 / 18656.0, 0},
+      {35.0 / 384.0, 0.0, 500.0 / 1113.0, 125.0 / 192.0, -2187.0 / 6784.0, 11.0 / 84.0}};
+  const double* d = dense_weights();
   for (int i = 0; i < 4; ++i) {
-    out[i] = h00 * xb[i] + h10 * h * vb[i] + h01 * xa[i] + h11 * h * va[i];
-    out[4 + i] = h00 * vb[i] + h10 * h * ka[i] + h01 * va[i] + h11 * h * kb[i];
+    // stage velocity increments w_j - v = h sum_l B[j][l] k_l
+    double sw = 0.0, sk = 0.0;
+    for (int j = 0; j < 7; ++j) {
+      double dw = 0.0;
+      for (int l = 0; l < j && l < 6; ++l) dw = dw + B[j][l] * k[4 * l + i];
+      sw = sw + d[j] * (h * dw);
+      sk = sk + d[j] * k[4 * j + i];
+    }
+    D.y0[i] = xb[i];
+    D.r2[i] = xa[i] - xb[i];
+    D.r3[i] = h * vb[i] - D.r2[i];
+    D.r4[i] = D.r2[i] - h * va[i] - D.r3[i];
+    D.r5[i] = h * sw;
+    D.y0[4 + i] = vb[i];
+    D.r2[4 + i] = va[i] - vb[i];
+    D.r3[4 + i] = h * k[i] - D.r2[4 + i];
+    D.r4[4 + i] = D.r2[4 + i] - h * k[24 + i] - D.r3[4 + i];
+    D.r5[4 + i] = h * sk;
   }
 }
 
-// EXTENSION: fraction s in [0, 1] where component c of the Hermite position
-// equals `target`, given the interpolant changes sign there.  Newton steps
-// from the chord's root, kept inside a shrinking bracket (bisection when a
-// Newton step leaves it); 30 iterations bound the loop.
-inline double hermite_root(const double xb[4], const double vb[4], const double xa[4],
-                           const double va[4], double h, int c, double target) {
-  auto f = [&](double s, double* df) {
-    const double s2 = s * s, s3 = s2 * s;
-    const double p = (2.0 * s3 - 3.0 * s2 + 1.0) * xb[c] + (s3 - 2.0 * s2 + s) * h * vb[c] +
-                     (-2.0 * s3 + 3.0 * s2) * xa[c] + (s3 - s2) * h * va[c];
-    *df = (6.0 * s2 - 6.0 * s) * xb[c] + (3.0 * s2 - 4.0 * s + 1.0) * h * vb[c] +
-          (-6.0 * s2 + 6.0 * s) * xa[c] + (3.0 * s2 - 2.0 * s) * h * va[c];
-    return p - target;
-  };
-  double lo = 0.0, hi = 1.0, dlo, dhi;
-  const double flo = f(lo, &dlo);
-  const double fhi = f(hi, &dhi);
+inline double dense_comp(const DenseStep& D, int c, double s) {
+  const double t = 1.0 - s;
+  return D.y0[c] + s * (D.r2[c] + t * (D.r3[c] + s * (D.r4[c] + t * D.r5[c])));
+}
+
+// d/ds of dense_comp
+inline double dense_slope(const DenseStep& D, int c, double s) {
+  const double t = 1.0 - s;
+  return D.r2[c] + (1.0 - 2.0 * s) * D.r3[c] + s * (2.0 - 3.0 * s) * D.r4[c] +
+         2.0 * s * t * (1.0 - 2.0 * s) * D.r5[c];
+}
+
+inline void dense_point(const DenseStep& D, double s, double out[8]) {
+  for (int c = 0; c < 8; ++c) out[c] = dense_comp(D, c, s);
+}
+
+// EXTENSION: fraction s in [0, 1] where component c of the continuous
+// extension equals `target`, given that it changes sign across the step:
+// Newton steps from the chord's root, kept inside a shrinking bracket
+// (bisection when a Newton step leaves it); 30 iterations bound the loop.
+inline double dense_root(const DenseStep& D, int c, double target) {
+  const double flo = dense_comp(D, c, 0.0) - target;
+  const double fhi = dense_comp(D, c, 1.0) - target;
+  double lo = 0.0, hi = 1.0;
   double s = flo / (flo - fhi);
   if (!(s >= 0.0 && s <= 1.0)) s = 0.5;
   for (int it = 0; it < 30; ++it) {
-    double d;
-    const double fs = f(s, &d);
+    const double fs = dense_comp(D, c, s) - target;
     if (fs == 0.0) break;
     if ((fs < 0.0) == (flo < 0.0)) lo = s; else hi = s;
+    const double d = dense_slope(D, c, s);
     double sn = d != 0.0 ? s - fs / d : 0.5 * (lo + hi);
     if (!(sn > lo && sn < hi)) sn = 0.5 * (lo + hi);
     if (std::fabs(sn - s) <= 1e-15) {
@@ -1013,7 +1059,14 @@ void shade(const M&, const TraceSetup& S, Sample& o) {  // renderer.rs:44-53
     case kClsHorizon: o.rgb[0] = o.rgb[1] = o.rgb[2] = 0.0; break;
     case kClsEscaped:
       if (S.sky == kSkyChecker) {
-        checker_sky(o.st.position[2], o.st.position[3], S.sky_rows, S.sky_cols, S.sky_seed, o.rgb);
+        // EXTENSION: with the full Dormand-Prince stepper (thin disk or none)
+        // the cell is read where the ray met the escape sphere, a point that
+        // does not depend on how far the last step overshot it
+        const bool at_cross = S.integ.stepper == 1 && S.disk_kind != kDiskVolumetric &&
+                              std::isfinite(o.cross[2]);
+        const double th = at_cross ? o.cross[2] : o.st.position[2];
+        const double ph = at_cross ? o.cross[3] : o.st.position[3];
+        checker_sky(th, ph, S.sky_rows, S.sky_cols, S.sky_seed, o.rgb);
       } else {
         procedural_sky(spatial_dir(o.st.velocity), o.rgb);
       }
@@ -1049,7 +1102,7 @@ Sample trace(const M& metric, const TraceSetup& S, const V4<double>& observer,
     State<double> before = st;
     bool acc = false;
     double h_used = 0.0;
-    double ends[12];  // full DP: a at both ends, raw end position
+    double ends[32];  // full DP: the step's k_1..k_7 and raw end position
     StepResult result = S.integ.step(metric, st, h, &acc, &h_used, ends);
     o.attempts += 1;
     if (acc) o.accepted += 1;
@@ -1059,24 +1112,31 @@ Sample trace(const M& metric, const TraceSetup& S, const V4<double>& observer,
       // the raw (un-normalised) end of the step: the reference's Euler segment
       // (geodesic.rs:312), or the full Dormand-Prince solution
       V4<double> raw = before.position + dl * before.velocity;
-      if (dp45) raw = V4<double>{{ends[8], ends[9], ends[10], ends[11]}};
-      // state at fraction s of the step: exact on the Euler segment, cubic
-      // Hermite (EXTENSION) for the full Dormand-Prince step
+      if (dp45) raw = V4<double>{{ends[28], ends[29], ends[30], ends[31]}};
+      // state at fraction s of the step: exact on the Euler segment, the
+      // continuous extension (EXTENSION) for the full Dormand-Prince step
+      DenseStep dense;
+      bool dense_ready = false;
+      auto ensure_dense = [&]() {
+        if (!dense_ready)
+          dense_build(before.position.c, before.velocity.c, raw.c, st.velocity.c, ends, dl, dense);
+        dense_ready = true;
+      };
       auto point = [&](double s, double out[8]) {
         if (!dp45) {
           segment_point(before, raw, st.velocity, s, out);
           return;
         }
-        hermite_point(before.position.c, before.velocity.c, ends, raw.c, st.velocity.c,
-                      ends + 4, dl, s, out);
+        ensure_dense();
+        dense_point(dense, s, out);
         V4<double> p{{out[0], out[1], out[2], out[3]}};
         normalize_spherical_coords(p);
         for (int i = 0; i < 4; ++i) out[i] = p[i];
       };
       auto root = [&](int c, double target, double linear_s) {
-        return dp45 ? hermite_root(before.position.c, before.velocity.c, raw.c, st.velocity.c,
-                                   dl, c, target)
-                    : linear_s;
+        if (!dp45) return linear_s;
+        ensure_dense();
+        return dense_root(dense, c, target);
       };
       // escape-sphere crossing on this step (EXTENSION output)
       if (before.position[1] <= S.integ.max_radius && raw[1] > S.integ.max_radius) {

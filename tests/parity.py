@@ -5,6 +5,7 @@ from __future__ import annotations
 
 import numpy as np
 
+from gargantua_b200.accuracy import crossing_geo_err  # noqa: F401  (re-exported)
 from gargantua_b200.curved import Scene
 
 TWO_PI = 2.0 * np.pi
@@ -83,3 +84,42 @@ def compare(scene: Scene, g, o, oracle_mod, idx=None, max_excluded=0.005):
     strict = (e_gpu[same] <= REL).mean()
     return {"class_mismatch": int((~same).sum()), "excluded": int(len(suspects)),
             "within_1e-9": float(strict), "attempts_equal": float(att_same)}
+
+
+
+def fp32_amplification(scene, oracle_mod, index: int, ref_cross: np.ndarray,
+                       delta: float = 1e-7) -> float:
+    """How much the FP64 oracle amplifies an input perturbation at the FP32
+    rounding level: sample `index` re-shot with its image-plane point moved by
+    `delta` in u and in v, crossing-state change (crossing_geo_err against
+    ref_cross, the unperturbed crossing) over delta, the larger of the two.
+    A ray whose amplification is well above 1 cannot hold 1e-6 in any FP32
+    representation of its state; infinite when the perturbed ray ends
+    elsewhere."""
+    from gargantua_b200.accuracy import crossing_geo_err as geo
+    u, v = oracle_mod.sample_uv(scene, int(index))
+    worst = 0.0
+    for du, dv in ((delta, 0.0), (0.0, delta)):
+        c = np.asarray(oracle_mod.trace_uv(scene, u + du, v + dv).cross).reshape(8, 1)
+        if not np.isfinite(c[0, 0]):
+            return float("inf")
+        worst = max(worst, float(geo(c, ref_cross.reshape(8, 1))[0]) / delta)
+    return worst
+
+
+def mixed_report(scene, g_cross, o_cross, oracle_mod, index=None, tol=1e-6,
+                 min_amplification=3.0):
+    """Crossing-state error of a mixed-precision render against the oracle's
+    FP64 crossings, and the rays beyond `tol` that the oracle itself does not
+    amplify by more than `min_amplification` (those are the mixed form's own
+    failures; the rest are ill-conditioned at FP32 resolution)."""
+    index = np.arange(g_cross.shape[1]) if index is None else np.asarray(index)
+    m = np.isfinite(o_cross[0]) & np.isfinite(g_cross[0])
+    e = crossing_geo_err(g_cross[:, m], o_cross[:, m])
+    over = np.nonzero(e > tol)[0]
+    unexplained = [int(index[m][k]) for k in over
+                   if fp32_amplification(scene, oracle_mod, index[m][k], o_cross[:, m][:, k])
+                   <= min_amplification]
+    return {"rays": int(m.sum()), "p50": float(np.quantile(e, 0.5)),
+            "p99": float(np.quantile(e, 0.99)), "p99.9": float(np.quantile(e, 0.999)),
+            "over_tol": int(over.size), "unexplained": unexplained}

@@ -52,3 +52,30 @@ def test_planted_step_count_error_is_caught(oracle_mod, runs):
     bad.attempts[::100] += 1
     with pytest.raises(AssertionError):
         compare(scene, bad, o, oracle_mod)
+
+
+# ---- the mixed form's criterion (tests/test_mixed.py) ------------------------------
+def _dp45_subset(oracle_mod):
+    from gargantua_b200 import abi
+    scene = workloads.schwarzschild_thin_256(stepper=abi.GG_STEPPER_DP45)
+    idx = np.arange(0, scene.n_samples, 997, dtype=np.uint64)
+    return scene, idx, oracle_mod.trace_cross(scene, idx)
+
+
+def test_mixed_criterion_accepts_fp32_sized_noise(oracle_mod):
+    from parity import mixed_report
+    scene, idx, oc = _dp45_subset(oracle_mod)
+    noisy = oc * (1.0 + 3e-8 * np.random.default_rng(0).standard_normal(oc.shape))
+    rep = mixed_report(scene, noisy, oc, oracle_mod, index=idx)
+    assert rep["p99"] <= 1e-6 and rep["unexplained"] == []
+
+
+def test_mixed_criterion_flags_error_on_well_conditioned_rays(oracle_mod):
+    """A 5e-6 error planted in the radius of well-conditioned rays is not
+    excused as ill-conditioning."""
+    from parity import mixed_report
+    scene, idx, oc = _dp45_subset(oracle_mod)
+    bad = oc.copy()
+    bad[1, :5] *= 1.0 + 5e-6
+    rep = mixed_report(scene, bad, oc, oracle_mod, index=idx)
+    assert len(rep["unexplained"]) >= 4

@@ -202,7 +202,7 @@ def test_dp45_kerr_1080p_seeded_subset(renderer, oracle_mod):
     o = oracle_mod.trace_samples(scene, idx.astype(np.uint64))
     rep = compare(scene, g, o, oracle_mod, idx=idx.astype(np.int64))
     assert rep["within_1e-9"] > 0.999, rep
-    # the crossing state (escape sphere / disk plane) from the Hermite interpolant
+    # the crossing state (escape sphere / disk plane) from the continuous extension
     oc = oracle_mod.trace_cross(scene, idx.astype(np.uint64))
     gc = g.cross[:, idx]
     m = np.isfinite(oc[0]) & np.isfinite(gc[0])
