@@ -157,6 +157,11 @@ __device__ __noinline__ uint32_t mixed_crossings(const DevParams& P, const DevOu
   return 0;
 }
 
+// Deferred per-ray work of a lane (low bits) and its flags.
+constexpr uint32_t kPendHandOff = 1, kPendCross = 2, kPendFinish = 3, kPendKind = 0xf;
+constexpr uint32_t kPendEsc = 0x10, kPendDsk = 0x20;  // kPendCross: which crossings
+constexpr uint32_t kPendClsShift = 8;                  // kPendFinish: the class
+
 // BUDGET: the render has an attempt budget (its bookkeeping costs registers,
 // so renders without one run a variant that has none).
 template <int METRIC, int DISK, bool BUDGET>
@@ -179,6 +184,11 @@ __global__ void __launch_bounds__(kTraceBlock, kMixedMinBlocks)
   bool crossed = false;
   bool k1_valid = false;
   bool k7_pending = false;
+  // Per-ray work found during the attempts (hand-off, crossing, finish) is
+  // deferred to the top of the loop, where every lane of the warp that has
+  // some runs it together instead of one lane at a time mid-period.
+  uint32_t pend = 0;      // kPend* | flags
+  float pend_hf = 0.0f;   // kPendCross: the accepted step awaiting its crossing
 
   uint64_t wbase = 0;
   uint32_t wcount = 0;
@@ -186,6 +196,32 @@ __global__ void __launch_bounds__(kTraceBlock, kMixedMinBlocks)
   unsigned budget_pending = 0;
 
   for (;;) {
+    // ---- deferred per-ray work ---------------------------------------------
+    if (pend) {
+      const uint32_t kind = pend & kPendKind;
+      if (kind == kPendHandOff) {
+        hand_off(O, ctl, K, S, n_att, n_acc);
+      } else if (kind == kPendCross) {
+        const uint32_t ended = mixed_crossings<METRIC, DISK>(
+            P, O, K, S, pend_hf, (pend & kPendEsc) != 0, (pend & kPendDsk) != 0, n_att, n_acc, &bs);
+        if (ended) {
+          if (BUDGET) budget_pending += ended;
+        } else {
+          mixed_advance(S, K, pend_hf, k1_valid, k7_pending);
+          if (n_att >= P.max_steps) {
+            mixed_finish(P, O, K, S, kClsMaxSteps, n_att, n_acc, crossed, &bs);
+            if (BUDGET) budget_pending += n_att;
+          } else {
+            live = true;
+          }
+        }
+      } else {
+        mixed_finish(P, O, K, S, (int)(pend >> kPendClsShift), n_att, n_acc, crossed, &bs);
+        if (BUDGET) budget_pending += n_att;
+      }
+      pend = 0;
+    }
+
     // ---- refill lanes whose ray finished or was handed off ----------------
     unsigned need = __ballot_sync(kFull, !live);
     if (BUDGET && need && !wdone) {
@@ -241,7 +277,7 @@ __global__ void __launch_bounds__(kTraceBlock, kMixedMinBlocks)
       {
         const float r = K.comp(kSlotXh, 1), th = K.comp(kSlotXh, 2);
         if (r < P.band_r || th < P.pole_band || th > kPiHi - P.pole_band) {
-          hand_off(O, ctl, K, S, n_att, n_acc);
+          pend = kPendHandOff;
           live = false;
           continue;
         }
@@ -250,44 +286,38 @@ __global__ void __launch_bounds__(kTraceBlock, kMixedMinBlocks)
       float hf = 0.0f;
       const int res = attempt_dp45_mixed<METRIC>(P, S, K, k1_valid, k7_pending, acc, hf);
       n_att += 1;
-      int done_cls = -1;
       if (acc) {
         const float4 dx = K.get(kSlotDx);
-        const float4 xh = K.get(kSlotXh), xl = K.get(kSlotXl);
-        const float th_a = xh.z + dx.z;
+        const float xh_r = K.comp(kSlotXh, 1), xh_th = K.comp(kSlotXh, 2);
+        const float th_a = xh_th + dx.z;
         if (!(th_a > 0.0f && th_a < kPiHi)) {
           // theta would turn through a pole: re-take this step in FP64
           n_att -= 1;
-          hand_off(O, ctl, K, S, n_att, n_acc);
+          pend = kPendHandOff;
           live = false;
           continue;
         }
         n_acc += 1;
-        const float dr_b = ff_minus(xh.y, xl.y, P.max_radius_hi, P.max_radius_lo);
+        const float dr_b = ff_minus(xh_r, K.comp(kSlotXl, 1), P.max_radius_hi, P.max_radius_lo);
         const bool esc = dr_b <= 0.0f && dr_b + dx.y > 0.0f;
         bool dsk = false;
         if (DISK == kDiskThin) {
-          const float d_b = ff_minus(xh.z, xl.z, kHalfPiHi, kHalfPiLo);
+          const float d_b = ff_minus(xh_th, K.comp(kSlotXl, 2), kHalfPiHi, kHalfPiLo);
           const float d_a = d_b + dx.z;
           dsk = (d_b < 0.0f && d_a >= 0.0f) || (d_b > 0.0f && d_a <= 0.0f);
         }
         if (esc || dsk) {
           if (esc && O.cross) crossed = true;
-          const uint32_t ended =
-              mixed_crossings<METRIC, DISK>(P, O, K, S, hf, esc, dsk, n_att, n_acc, &bs);
-          if (ended) {
-            if (BUDGET) budget_pending += ended;
-            live = false;
-            continue;
-          }
+          pend = kPendCross | (esc ? kPendEsc : 0u) | (dsk ? kPendDsk : 0u);
+          pend_hf = hf;
+          live = false;
+          continue;
         }
         mixed_advance(S, K, hf, k1_valid, k7_pending);
       }
-      if (res == kEscaped) done_cls = kClsEscaped;
-      else if (n_att >= P.max_steps) done_cls = kClsMaxSteps;
-      if (done_cls >= 0) {
-        mixed_finish(P, O, K, S, done_cls, n_att, n_acc, crossed, &bs);
-        if (BUDGET) budget_pending += n_att;
+      if (res == kEscaped || n_att >= P.max_steps) {
+        pend = kPendFinish | ((uint32_t)(res == kEscaped ? kClsEscaped : kClsMaxSteps)
+                              << kPendClsShift);
         live = false;
       }
     }
