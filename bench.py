@@ -21,6 +21,11 @@ against the FP64 kernel on every sample.  ``e2e`` is the headline metric
 through the public synchronous call ``gg_render`` into pinned host memory
 (parameters in, sRGB image out, copies inside the timed region).
 
+``--workload stress`` runs the near-extremal stress configuration instead (Kerr
+a = 0.998, 4096 x 4096 x 16 jittered samples, camera r = 15 M at 85 deg, disk
+r_ISCO-25 M, 50,000 step() calls): one frame per form and the distribution of
+per-ray attempts, as a separate JSON line.
+
 ``--impl reference`` times the CPU restatement of the reference's renderer
 (the oracle; the Rust reference cannot be built here) on the host cores on
 a bounded seeded sample of the same frame.
@@ -28,6 +33,7 @@ a bounded seeded sample of the same frame.
 from __future__ import annotations
 
 import argparse
+import ctypes as C
 import json
 import os
 import statistics
@@ -317,6 +323,82 @@ def run_ours(args) -> None:
         print(json.dumps(line), flush=True)
 
 
+# ---- stress configuration ------------------------------------------------------------
+def run_stress(args) -> None:
+    """Near-extremal Kerr a = 0.998, side x side pixels x spp seeded jittered
+    samples (default 4096 x 4096 x 16), camera r = 15 M at 85 deg, disk
+    r_ISCO-25 M, 50,000 step() calls per ray: one frame per form (plain FP64,
+    FP64 full Dormand-Prince, mixed), timed with CUDA events after a warm-up
+    frame of 256 x 256 x 1, and the per-ray attempt distribution.  Per-ray
+    outputs stay on the device (attempts and class only)."""
+    import torch
+
+    from gargantua_b200 import abi, workloads
+    from gargantua_b200.curved import Renderer
+
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    r = Renderer(local)
+    side, spp = args.side, args.spp
+    n = side * side * spp
+    img = torch.empty(side * side * 3, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.ExternalStream(r.stream)
+    edges = [0] + [2 ** k for k in range(17)]  # attempts per ray: [0,1), [1,2), [2,4), ...
+    forms, cls_of = {}, {}
+    for form, prec, stepper in (("fp64", abi.GG_PREC_FP64, abi.GG_STEPPER_REFERENCE),
+                                ("fp64_dp45", abi.GG_PREC_FP64, abi.GG_STEPPER_DP45),
+                                ("mixed", abi.GG_PREC_MIXED, abi.GG_STEPPER_DP45)):
+        warm = workloads.kerr_stress_4k(precision=prec, side=256, spp=1, stepper=stepper)
+        r.render_device(warm, img.data_ptr(), None, r.stream)
+        scene = workloads.kerr_stress_4k(precision=prec, side=side, spp=spp, stepper=stepper)
+        att = torch.empty(n, dtype=torch.int32, device="cuda")
+        cls = torch.empty(n, dtype=torch.int32, device="cuda")
+        rays = abi.gg_ray_out_t()
+        rays.attempts = C.cast(C.c_void_p(att.data_ptr()), C.POINTER(C.c_uint32))
+        rays.cls = C.cast(C.c_void_p(cls.data_ptr()), C.POINTER(C.c_int32))
+        stream.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r.render_device(scene, img.data_ptr(), rays, r.stream)
+        e1.record(stream)
+        stream.synchronize()
+        ms = e0.elapsed_time(e1)
+        st = r.stats()
+        a = att.to(torch.int64)
+        hist = [int(((a >= lo) & (a < hi)).sum()) for lo, hi in zip(edges[:-1], edges[1:])]
+        hist.append(int((a >= edges[-1]).sum()))
+        q = torch.quantile(a[:: max(1, n // 4_000_000)].double(),
+                           torch.tensor([0.5, 0.9, 0.99, 0.999], dtype=torch.float64,
+                                        device="cuda")).tolist()
+        forms[form] = {"ms": ms, "geodesics_per_s": n / (ms * 1e-3),
+                       "attempts": int(st.attempts), "accepted": int(st.accepted),
+                       "attempts_per_s": st.attempts / (ms * 1e-3),
+                       "class_count": [int(x) for x in st.class_count],
+                       "fp64_band_rays": int(st.fp64_rays),
+                       "fp64_band_attempts": int(st.fp64_attempts),
+                       "attempts_per_ray": {"p50": q[0], "p90": q[1], "p99": q[2], "p99.9": q[3],
+                                            "max": int(a.max())},
+                       "attempts_histogram": {"bin_lower_edges": edges[:-1] + [edges[-1]],
+                                              "counts": hist}}
+        cls_of[form] = cls
+        del att
+    line = {"metric": "Kerr a=0.998 4096^2 x16 spp stress: geodesics/s and per-ray steps",
+            "unit": UNIT, "n_gpus": 1, "higher_is_better": True,
+            "config": {"workload": f"kerr_a0.998_{side}x{side}x{spp}spp_thin_disk",
+                       "r_cam": 15.0, "inclination_deg": 85.0, "disk": "r_ISCO-25M",
+                       "max_steps": 50000, "rtol": 1e-8, "atol": 1e-10, "samples": n},
+            "forms": forms,
+            "mixed_over_fp64": forms["mixed"]["geodesics_per_s"] / forms["fp64"]["geodesics_per_s"],
+            "mixed_over_fp64_dp45": (forms["mixed"]["geodesics_per_s"]
+                                     / forms["fp64_dp45"]["geodesics_per_s"]),
+            "class_agreement_mixed_vs_fp64_dp45":
+                float((cls_of["mixed"] == cls_of["fp64_dp45"]).double().mean())}
+    r.close()
+    print(json.dumps(line), flush=True)
+
+
 # ---- reference arm ---------------------------------------------------------------
 def run_reference(args) -> None:
     import numpy as np
@@ -369,9 +451,15 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=["kerr1080p", "stress"], default="kerr1080p",
+                    help="stress: the a=0.998 4096^2 x 16 spp configuration (one frame per form)")
+    ap.add_argument("--side", type=int, default=4096, help="stress: image side")
+    ap.add_argument("--spp", type=int, default=16, help="stress: samples per pixel")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "stress":
+        run_stress(args)
     else:
         run_ours(args)
 
