@@ -35,6 +35,7 @@ GG_PREC_FP64 = 0
 GG_PREC_MIXED = 1
 GG_STEPPER_REFERENCE = 0
 GG_STEPPER_DP45 = 1
+GG_BATCH_VARIANTS = 6
 GG_SKY_PROCEDURAL = 0
 GG_SKY_CHECKER = 1
 
@@ -85,6 +86,11 @@ class gg_ray_out_t(C.Structure):
                 ("rgb", C.POINTER(C.c_double)), ("cross", C.POINTER(C.c_double))]
 
 
+class gg_scene_t(C.Structure):
+    _fields_ = [("metric", gg_metric_t), ("camera", gg_camera_t), ("disk", gg_disk_t),
+                ("width", C.c_uint32), ("height", C.c_uint32), ("sky_seed", C.c_uint64)]
+
+
 class gg_stats_t(C.Structure):
     _fields_ = [("rays", C.c_uint64), ("attempts", C.c_uint64), ("accepted", C.c_uint64),
                 ("class_count", C.c_uint64 * 5), ("kernel_ms", C.c_double),
@@ -98,6 +104,7 @@ STRUCTS = {
     "gg_integrator_t": gg_integrator_t,
     "gg_render_opts_t": gg_render_opts_t,
     "gg_ray_out_t": gg_ray_out_t,
+    "gg_scene_t": gg_scene_t,
     "gg_stats_t": gg_stats_t,
 }
 
@@ -130,6 +137,14 @@ _SIGNATURES = {
                                    C.c_uint32, C.c_void_p, P(gg_ray_out_t), C.c_void_p]),
     "gg_measure_fma_peak": (C.c_int, [C.c_void_p, C.c_int, P(C.c_double)]),
     "gg_polar_sincos": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32]),
+    "gg_render_batch": (C.c_int, [C.c_void_p, P(gg_scene_t), C.c_uint32, P(gg_integrator_t),
+                                  P(gg_render_opts_t), C.c_void_p]),
+    "gg_render_batch_device": (C.c_int, [C.c_void_p, P(gg_scene_t), C.c_uint32,
+                                         P(gg_integrator_t), P(gg_render_opts_t), C.c_void_p,
+                                         C.c_void_p]),
+    "gg_batch_autotune": (C.c_int, [C.c_void_p, P(gg_scene_t), C.c_uint32, P(gg_integrator_t),
+                                    P(gg_render_opts_t), P(C.c_int), P(C.c_double)]),
+    "gg_batch_set_variant": (C.c_int, [C.c_void_p, C.c_int]),
     "gg_render_device_noalloc": (C.c_int, [P(gg_metric_t), P(gg_camera_t), P(gg_disk_t),
                                            P(gg_integrator_t), P(gg_render_opts_t), C.c_uint32,
                                            C.c_uint32, C.c_void_p, P(gg_ray_out_t),

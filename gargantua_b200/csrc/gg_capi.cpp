@@ -35,6 +35,24 @@ struct gg_ctx {
   size_t staging_cap = 0;
   void* queue = nullptr;           // mixed form: rays handed to the FP64 pass
   size_t queue_cap = 0;
+  // batched renders: scene table (device and pinned host mirror), kernel
+  // variant, and the cached graph of the last batch shape
+  void* batch_dev = nullptr;
+  size_t batch_dev_cap = 0;
+  void* batch_host = nullptr;
+  size_t batch_host_cap = 0;
+  int batch_variant = 0;
+  struct BatchKey {
+    uint32_t n = 0;
+    uint64_t total = 0;
+    int variant = -1;
+    const void* queue = nullptr;
+    const void* table = nullptr;
+    gg_integrator_t integ{};
+    gg_render_opts_t opts{};
+    int metric = -1, disk = -1;
+  } batch_key;
+  cudaGraphExec_t batch_exec = nullptr;
   bool pending = false;            // stats of the last device-pointer render not read yet
   gg_stats_t last{};
   std::mutex mu;
@@ -292,6 +310,21 @@ void build_params(const gg_metric_t* metric, const gg_camera_t* camera, const gg
   *out = P;
 }
 
+int grow_pinned(void** buf, size_t* cap, size_t need) {
+  if (need <= *cap) return GG_OK;
+  if (*buf) cudaFreeHost(*buf);
+  *buf = nullptr;
+  *cap = 0;
+  const size_t want = need + need / 4;
+  if (cudaMallocHost(buf, want) != cudaSuccess) {
+    cudaGetLastError();
+    *buf = nullptr;
+    return GG_ERR_OOM;
+  }
+  *cap = want;
+  return GG_OK;
+}
+
 int grow(void** buf, size_t* cap, size_t need) {
   if (need <= *cap) return GG_OK;
   if (*buf) cudaFree(*buf);
@@ -395,6 +428,164 @@ struct Lock {
   std::lock_guard<std::mutex> g;
 };
 
+// ---- batched renders --------------------------------------------------------
+struct BatchLaunch {
+  DevParams P0;  // the batch's common parameters (integrator, sky kind), n_rays = total
+  DevOutputs O0;  // the FP64 band queue
+  gg::BatchTable table;
+  size_t table_bytes = 0;  // bytes of the scene table + prefix array to upload
+  uint64_t total = 0;
+  uint64_t pixels = 0;
+  int grid = 0, qgrid = 0;
+};
+
+// Validates the batch, writes the scene table (per-scene parameters and
+// image pointers into rgb_dev, prefix sums of sample counts) to the pinned
+// mirror, grows the device table and the band queue, and sizes the grids.
+int batch_prepare(gg_ctx* c, const gg_scene_t* scenes, uint32_t n, const gg_integrator_t* integ,
+                  const gg_render_opts_t* opts, uint8_t* rgb_dev, int variant, BatchLaunch* L) {
+  if (!scenes || n == 0 || !integ || !opts) return GG_ERR_INVALID_ARG;
+  if (integ->precision != GG_PREC_MIXED || integ->stepper != GG_STEPPER_DP45)
+    return GG_ERR_UNSUPPORTED;
+  if (opts->samples_per_axis > 1 || opts->jitter_spp > 0 || opts->attempt_budget != 0)
+    return GG_ERR_UNSUPPORTED;
+  const int kind = scenes[0].metric.kind, disk_kind = scenes[0].disk.kind;
+  if (disk_kind != GG_DISK_NONE && disk_kind != GG_DISK_THIN) return GG_ERR_UNSUPPORTED;
+  for (uint32_t k = 0; k < n; ++k) {
+    if (scenes[k].metric.kind != kind || scenes[k].disk.kind != disk_kind)
+      return GG_ERR_UNSUPPORTED;
+    gg_render_opts_t o = *opts;
+    o.sky_seed = scenes[k].sky_seed;
+    const gg_disk_t* d = disk_kind == GG_DISK_NONE ? nullptr : &scenes[k].disk;
+    const int v = validate(&scenes[k].metric, &scenes[k].camera, d, integ, &o, scenes[k].width,
+                           scenes[k].height);
+    if (v != GG_OK) return v;
+  }
+  const size_t off_first = align256(sizeof(gg::BatchScene) * n);
+  L->table_bytes = off_first + sizeof(uint64_t) * (n + 1);
+  int st = grow_pinned(&c->batch_host, &c->batch_host_cap, L->table_bytes);
+  if (st != GG_OK) return st;
+  st = grow(&c->batch_dev, &c->batch_dev_cap, L->table_bytes);
+  if (st != GG_OK) return st;
+  auto* T = static_cast<gg::BatchScene*>(c->batch_host);
+  auto* first = reinterpret_cast<uint64_t*>(static_cast<char*>(c->batch_host) + off_first);
+  uint64_t total = 0, pix = 0;
+  for (uint32_t k = 0; k < n; ++k) {
+    gg_render_opts_t o = *opts;
+    o.sky_seed = scenes[k].sky_seed;
+    const gg_disk_t* d = disk_kind == GG_DISK_NONE ? nullptr : &scenes[k].disk;
+    build_params(&scenes[k].metric, &scenes[k].camera, d, integ, &o, scenes[k].width,
+                 scenes[k].height, &T[k].P);
+    std::memset(&T[k].O, 0, sizeof(T[k].O));
+    T[k].O.rgb8 = rgb_dev ? rgb_dev + 3 * pix : nullptr;
+    first[k] = total;
+    total += T[k].P.n_rays;
+    pix += (uint64_t)scenes[k].width * scenes[k].height;
+  }
+  first[n] = total;
+  L->total = total;
+  L->pixels = pix;
+  L->P0 = T[0].P;
+  L->P0.n_rays = total;
+  st = grow(&c->queue, &c->queue_cap, sizeof(gg::QueuedRay) * total);
+  if (st != GG_OK) return st;
+  std::memset(&L->O0, 0, sizeof(L->O0));
+  L->O0.queue = static_cast<gg::QueuedRay*>(c->queue);
+  L->O0.queue_cap = total;
+  L->table.scenes = static_cast<const gg::BatchScene*>(c->batch_dev);
+  L->table.first = reinterpret_cast<const uint64_t*>(static_cast<char*>(c->batch_dev) + off_first);
+  L->table.n = n;
+  int bps = 0, qbps = 0;
+  if (gg::mixed_occupancy(L->P0, &bps, &L->table, variant) != cudaSuccess || bps < 1)
+    return GG_ERR_CUDA;
+  if (gg::queue_trace_occupancy(L->P0, &qbps) != cudaSuccess || qbps < 1) return GG_ERR_CUDA;
+  uint64_t grid = (uint64_t)c->sms * bps;
+  const uint64_t need_blocks = (total + gg::kTraceBlock - 1) / gg::kTraceBlock;
+  if (grid > need_blocks) grid = need_blocks;
+  L->grid = (int)(grid < 1 ? 1 : grid);
+  L->qgrid = c->sms * qbps;
+  return GG_OK;
+}
+
+// The batch's device work on `s`: upload the table, reset the counters, the
+// mixed launch, the FP64 band pass, the counters back to the pinned mirror.
+// Runs directly, or under stream capture to build the batch graph.
+int batch_body(gg_ctx* c, const BatchLaunch& L, int variant, cudaStream_t s) {
+  if (cudaMemcpyAsync(c->batch_dev, c->batch_host, L.table_bytes, cudaMemcpyHostToDevice, s) !=
+      cudaSuccess)
+    return GG_ERR_CUDA;
+  if (cudaMemsetAsync(c->ctl, 0, sizeof(DevControl), s) != cudaSuccess) return GG_ERR_CUDA;
+  if (gg::launch_mixed(L.P0, L.O0, c->ctl, L.grid, s, &L.table, variant) != cudaSuccess)
+    return GG_ERR_CUDA;
+  if (gg::launch_queue_trace(L.P0, L.O0, c->ctl, L.qgrid, s, &L.table) != cudaSuccess)
+    return GG_ERR_CUDA;
+  if (cudaMemcpyAsync(c->ctl_host, c->ctl, sizeof(DevControl), cudaMemcpyDeviceToHost, s) !=
+      cudaSuccess)
+    return GG_ERR_CUDA;
+  return GG_OK;
+}
+
+// One batched render into rgb_dev on `stream` through the cached graph.
+int batch_render(gg_ctx* c, const gg_scene_t* scenes, uint32_t n, const gg_integrator_t* integ,
+                 const gg_render_opts_t* opts, uint8_t* rgb_dev, cudaStream_t stream) {
+  // the pinned table is rewritten: the previous render must have read it
+  if (cudaEventSynchronize(c->ev_done) != cudaSuccess) return GG_ERR_CUDA;
+  const int variant = c->batch_variant;
+  BatchLaunch L;
+  int st = batch_prepare(c, scenes, n, integ, opts, rgb_dev, variant, &L);
+  if (st != GG_OK) return st;
+  gg_ctx::BatchKey key;
+  key.n = n;
+  key.total = L.total;
+  key.variant = variant;
+  key.queue = c->queue;
+  key.table = c->batch_dev;
+  key.integ = *integ;
+  key.opts = *opts;
+  key.opts.sky_seed = 0;
+  key.metric = scenes[0].metric.kind;
+  key.disk = scenes[0].disk.kind;
+  const bool same = c->batch_exec && key.n == c->batch_key.n &&
+                    key.total == c->batch_key.total && key.variant == c->batch_key.variant &&
+                    key.queue == c->batch_key.queue && key.table == c->batch_key.table &&
+                    key.metric == c->batch_key.metric && key.disk == c->batch_key.disk &&
+                    std::memcmp(&key.integ, &c->batch_key.integ, sizeof(key.integ)) == 0 &&
+                    std::memcmp(&key.opts, &c->batch_key.opts, sizeof(key.opts)) == 0;
+  if (!same) {
+    if (c->batch_exec) cudaGraphExecDestroy(c->batch_exec);
+    c->batch_exec = nullptr;
+    if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+      return GG_ERR_CUDA;
+    st = batch_body(c, L, variant, c->stream);
+    cudaGraph_t g = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
+    if (st != GG_OK || ce != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      return st != GG_OK ? st : GG_ERR_CUDA;
+    }
+    const cudaError_t ie = cudaGraphInstantiate(&c->batch_exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) {
+      c->batch_exec = nullptr;
+      return GG_ERR_CUDA;
+    }
+    c->batch_key = key;
+  }
+  if (cudaEventRecord(c->ev_start, stream) != cudaSuccess) return GG_ERR_CUDA;
+  if (cudaGraphLaunch(c->batch_exec, stream) != cudaSuccess) return GG_ERR_CUDA;
+  if (cudaEventRecord(c->ev_stop, stream) != cudaSuccess) return GG_ERR_CUDA;
+  if (cudaEventRecord(c->ev_done, stream) != cudaSuccess) return GG_ERR_CUDA;
+  c->pending = true;
+  return GG_OK;
+}
+
+uint64_t batch_pixels(const gg_scene_t* scenes, uint32_t n) {
+  uint64_t p = 0;
+  for (uint32_t k = 0; k < n; ++k) p += (uint64_t)scenes[k].width * scenes[k].height;
+  return p;
+}
+
 }  // namespace
 
 namespace gg {
@@ -443,6 +634,7 @@ GG_API int gg_struct_size(const char* name) {
            {"gg_render_opts_t", (int)sizeof(gg_render_opts_t)},
            {"gg_ray_out_t", (int)sizeof(gg_ray_out_t)},
            {"gg_stats_t", (int)sizeof(gg_stats_t)},
+           {"gg_scene_t", (int)sizeof(gg_scene_t)},
            // bytes that reach the device per render as kernel parameters
            {"launch_params", (int)(sizeof(DevParams) + sizeof(DevOutputs) + sizeof(void*))}};
   for (auto& e : t)
@@ -580,6 +772,9 @@ GG_API int gg_destroy(gg_ctx* c) {
   if (c->samples) cudaFree(c->samples);
   if (c->staging) cudaFree(c->staging);
   if (c->queue) cudaFree(c->queue);
+  if (c->batch_exec) cudaGraphExecDestroy(c->batch_exec);
+  if (c->batch_dev) cudaFree(c->batch_dev);
+  if (c->batch_host) cudaFreeHost(c->batch_host);
   if (c->ctl) cudaFree(c->ctl);
   if (c->ctl_host) cudaFreeHost(c->ctl_host);
   if (c->ev_start) cudaEventDestroy(c->ev_start);
@@ -636,6 +831,87 @@ GG_API int gg_render_device(gg_ctx* c, const gg_metric_t* metric, const gg_camer
   O.rgb8 = rgb_dev;
   // NULL is CUDA's default stream, as for any CUDA API taking a stream
   return enqueue(c, P, O, rgb_dev != nullptr, static_cast<cudaStream_t>(stream));
+}
+
+GG_API int gg_render_batch_device(gg_ctx* c, const gg_scene_t* scenes, uint32_t n,
+                                  const gg_integrator_t* integ, const gg_render_opts_t* opts,
+                                  uint8_t* rgb_dev, void* stream) {
+  if (!c || !rgb_dev) return GG_ERR_INVALID_ARG;
+  Lock lock(c);
+  return batch_render(c, scenes, n, integ, opts, rgb_dev, static_cast<cudaStream_t>(stream));
+}
+
+GG_API int gg_render_batch(gg_ctx* c, const gg_scene_t* scenes, uint32_t n,
+                           const gg_integrator_t* integ, const gg_render_opts_t* opts,
+                           uint8_t* const* rgb_out) {
+  if (!c || !scenes || n == 0 || !rgb_out) return GG_ERR_INVALID_ARG;
+  for (uint32_t k = 0; k < n; ++k)
+    if (!rgb_out[k]) return GG_ERR_INVALID_ARG;
+  Lock lock(c);
+  if (cudaEventSynchronize(c->ev_done) != cudaSuccess) return GG_ERR_CUDA;  // staging reuse
+  int st = grow(&c->staging, &c->staging_cap, 3 * batch_pixels(scenes, n));
+  if (st != GG_OK) return st;
+  uint8_t* dev = static_cast<uint8_t*>(c->staging);
+  st = batch_render(c, scenes, n, integ, opts, dev, c->stream);
+  if (st != GG_OK) return st;
+  uint64_t off = 0;
+  for (uint32_t k = 0; k < n; ++k) {
+    const size_t bytes = 3ull * scenes[k].width * scenes[k].height;
+    if (cudaMemcpyAsync(rgb_out[k], dev + off, bytes, cudaMemcpyDeviceToHost, c->stream) !=
+        cudaSuccess)
+      return GG_ERR_CUDA;
+    off += bytes;
+  }
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return GG_ERR_CUDA;
+  return collect(c);
+}
+
+static_assert(GG_BATCH_VARIANTS == gg::kBatchVariants, "batch variant count");
+
+GG_API int gg_batch_autotune(gg_ctx* c, const gg_scene_t* scenes, uint32_t n,
+                             const gg_integrator_t* integ, const gg_render_opts_t* opts,
+                             int* variant_out, double* ms_out) {
+  if (!c || !scenes || n == 0) return GG_ERR_INVALID_ARG;
+  Lock lock(c);
+  if (cudaEventSynchronize(c->ev_done) != cudaSuccess) return GG_ERR_CUDA;
+  int st = grow(&c->staging, &c->staging_cap, 3 * batch_pixels(scenes, n));
+  if (st != GG_OK) return st;
+  uint8_t* dev = static_cast<uint8_t*>(c->staging);
+  int best = 0;
+  double best_ms = 1e300;
+  for (int v = 0; v < GG_BATCH_VARIANTS; ++v) {
+    double vms = 1e300;
+    for (int rep = 0; rep < 2; ++rep) {  // the first run of a variant also loads its code
+      BatchLaunch L;
+      st = batch_prepare(c, scenes, n, integ, opts, dev, v, &L);
+      if (st != GG_OK) return st;
+      if (cudaEventRecord(c->ev_start, c->stream) != cudaSuccess) return GG_ERR_CUDA;
+      st = batch_body(c, L, v, c->stream);
+      if (st != GG_OK) return st;
+      if (cudaEventRecord(c->ev_stop, c->stream) != cudaSuccess) return GG_ERR_CUDA;
+      if (cudaStreamSynchronize(c->stream) != cudaSuccess) return GG_ERR_CUDA;
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, c->ev_start, c->ev_stop) != cudaSuccess) return GG_ERR_CUDA;
+      if (ms < vms) vms = ms;
+    }
+    if (ms_out) ms_out[v] = vms;
+    if (vms < best_ms) {
+      best_ms = vms;
+      best = v;
+    }
+  }
+  c->batch_variant = best;
+  c->pending = false;
+  cudaEventRecord(c->ev_done, c->stream);
+  if (variant_out) *variant_out = best;
+  return GG_OK;
+}
+
+GG_API int gg_batch_set_variant(gg_ctx* c, int variant) {
+  if (!c || variant < 0 || variant >= GG_BATCH_VARIANTS) return GG_ERR_INVALID_ARG;
+  Lock lock(c);
+  c->batch_variant = variant;
+  return GG_OK;
 }
 
 GG_API int gg_render(gg_ctx* c, const gg_metric_t* metric, const gg_camera_t* camera,

@@ -40,12 +40,18 @@ cudaError_t launch_trace(const DevParams& P, const DevOutputs& O, DevControl* ct
 // Mixed form (P.precision == GG_PREC_MIXED, full Dormand-Prince): the FP32
 // pass over the samples, which hands FP64-band rays to O.queue, and the FP64
 // pass over that queue.
-cudaError_t mixed_occupancy(const DevParams& P, int* blocks_per_sm);
+// A batched render (batch != nullptr) runs one of kBatchVariants kernel
+// variants (compaction period x register budget), chosen by `variant`.
+constexpr int kBatchVariants = 6;
+cudaError_t mixed_occupancy(const DevParams& P, int* blocks_per_sm,
+                            const BatchTable* batch = nullptr, int variant = 0);
 cudaError_t launch_mixed(const DevParams& P, const DevOutputs& O, DevControl* ctl, int grid,
-                         cudaStream_t stream);
+                         cudaStream_t stream, const BatchTable* batch = nullptr,
+                         int variant = 0);
 cudaError_t queue_trace_occupancy(const DevParams& P, int* blocks_per_sm);
 cudaError_t launch_queue_trace(const DevParams& P, const DevOutputs& O, DevControl* ctl,
-                               int grid, cudaStream_t stream);
+                               int grid, cudaStream_t stream,
+                               const BatchTable* batch = nullptr);
 
 // Best-of-5 FMA throughput (FLOP/s, FMA = 2) of the current device.
 cudaError_t measure_fma_peak(int fp64, int sms, double* flops);

@@ -34,7 +34,8 @@ namespace {
 // ray).  The state is the one the next attempt starts from.  The register
 // part of the ray comes by value, so the stepping loop keeps it in registers.
 __device__ __noinline__ void hand_off(const DevOutputs& O, DevControl* ctl, MixedSmem K,
-                                      MixedRegs S, uint32_t n_att, uint32_t n_acc) {
+                                      MixedRegs S, uint32_t n_att, uint32_t n_acc,
+                                      uint32_t scene) {
   const unsigned long long slot = atomicAdd(&ctl->queued, 1ull);
   if (slot >= O.queue_cap) {
     atomicExch(&ctl->queue_overflow, 1u);
@@ -52,6 +53,17 @@ __device__ __noinline__ void hand_off(const DevOutputs& O, DevControl* ctl, Mixe
   q.idx = K.idx();
   q.n_att = n_att;
   q.n_acc = n_acc;
+  q.scene = scene;
+}
+
+// Scene of global sample g in a batched launch: the last k with first[k] <= g.
+GG_DEV uint32_t find_scene(const BatchTable& B, uint64_t g) {
+  uint32_t lo = 0, hi = B.n;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (B.first[mid] <= g) lo = mid; else hi = mid;
+  }
+  return lo;
 }
 
 // Writes a finished ray's outcome (its state converted to FP64) and counts it
@@ -163,11 +175,16 @@ constexpr uint32_t kPendEsc = 0x10, kPendDsk = 0x20;  // kPendCross: which cross
 constexpr uint32_t kPendClsShift = 8;                  // kPendFinish: the class
 
 // BUDGET: the render has an attempt budget (its bookkeeping costs registers,
-// so renders without one run a variant that has none).
-template <int METRIC, int DISK, bool BUDGET>
-__global__ void __launch_bounds__(kTraceBlock, kMixedMinBlocks)
+// so renders without one run a variant that has none).  BATCH: the samples
+// are the concatenated samples of many scenes (B); each lane looks up its
+// sample's scene, whose parameters and outputs replace P and O for that ray
+// (the integrator, sky kind and budget are the batch's, in P).  PERIOD
+// (attempts between refills) and MINB (CTAs per SM the registers are
+// budgeted for) are the settings the batch autotuner chooses between.
+template <int METRIC, int DISK, bool BUDGET, bool BATCH, int PERIOD, int MINB>
+__global__ void __launch_bounds__(kTraceBlock, MINB)
     trace_mixed_kernel(const __grid_constant__ DevParams P, const __grid_constant__ DevOutputs O,
-                       DevControl* ctl) {
+                       DevControl* ctl, const __grid_constant__ BatchTable B) {
   const unsigned lane = threadIdx.x & 31u;
   __shared__ BlockStats bs;
   __shared__ float4 k_smem[kMixedSlots][kTraceBlock];
@@ -179,6 +196,7 @@ __global__ void __launch_bounds__(kTraceBlock, kMixedMinBlocks)
   __syncthreads();
 
   MixedRegs S;
+  uint32_t scene = 0;  // BATCH: the ray's scene
   bool live = false;
   uint32_t n_att = 0, n_acc = 0;
   bool crossed = false;
@@ -198,25 +216,27 @@ __global__ void __launch_bounds__(kTraceBlock, kMixedMinBlocks)
   for (;;) {
     // ---- deferred per-ray work ---------------------------------------------
     if (pend) {
+      const DevParams& PL = BATCH ? B.scenes[scene].P : P;
+      const DevOutputs& OL = BATCH ? B.scenes[scene].O : O;
       const uint32_t kind = pend & kPendKind;
       if (kind == kPendHandOff) {
-        hand_off(O, ctl, K, S, n_att, n_acc);
+        hand_off(O, ctl, K, S, n_att, n_acc, scene);
       } else if (kind == kPendCross) {
         const uint32_t ended = mixed_crossings<METRIC, DISK>(
-            P, O, K, S, pend_hf, (pend & kPendEsc) != 0, (pend & kPendDsk) != 0, n_att, n_acc, &bs);
+            PL, OL, K, S, pend_hf, (pend & kPendEsc) != 0, (pend & kPendDsk) != 0, n_att, n_acc, &bs);
         if (ended) {
           if (BUDGET) budget_pending += ended;
         } else {
           mixed_advance(S, K, pend_hf, k1_valid, k7_pending);
-          if (n_att >= P.max_steps) {
-            mixed_finish(P, O, K, S, kClsMaxSteps, n_att, n_acc, crossed, &bs);
+          if (n_att >= PL.max_steps) {
+            mixed_finish(PL, OL, K, S, kClsMaxSteps, n_att, n_acc, crossed, &bs);
             if (BUDGET) budget_pending += n_att;
           } else {
             live = true;
           }
         }
       } else {
-        mixed_finish(P, O, K, S, (int)(pend >> kPendClsShift), n_att, n_acc, crossed, &bs);
+        mixed_finish(PL, OL, K, S, (int)(pend >> kPendClsShift), n_att, n_acc, crossed, &bs);
         if (BUDGET) budget_pending += n_att;
       }
       pend = 0;
@@ -255,8 +275,12 @@ __global__ void __launch_bounds__(kTraceBlock, kMixedMinBlocks)
       const unsigned take = nn < wcount ? nn : wcount;
       const unsigned rank = (unsigned)__popc(need & lanemask_lt());
       if (!live && rank < take) {
-        const uint64_t idx = wbase + rank;
-        mixed_load(start_sample(P, idx), idx, K, S);
+        uint64_t idx = wbase + rank;
+        if (BATCH) {
+          scene = find_scene(B, idx);
+          idx -= B.first[scene];
+        }
+        mixed_load(start_sample(BATCH ? B.scenes[scene].P : P, idx), idx, K, S);
         live = true;
         n_att = 0;
         n_acc = 0;
@@ -272,11 +296,12 @@ __global__ void __launch_bounds__(kTraceBlock, kMixedMinBlocks)
 
     // ---- advance every live ray by up to kPeriod attempts -----------------
 #pragma unroll 1
-    for (int it = 0; it < kPeriod; ++it) {
+    for (int it = 0; it < PERIOD; ++it) {
       if (!live) continue;
+      const DevParams& PL = BATCH ? B.scenes[scene].P : P;
       {
         const float r = K.comp(kSlotXh, 1), th = K.comp(kSlotXh, 2);
-        if (r < P.band_r || th < P.pole_band || th > kPiHi - P.pole_band) {
+        if (r < PL.band_r || th < PL.pole_band || th > kPiHi - PL.pole_band) {
           pend = kPendHandOff;
           live = false;
           continue;
@@ -284,7 +309,7 @@ __global__ void __launch_bounds__(kTraceBlock, kMixedMinBlocks)
       }
       bool acc;
       float hf = 0.0f;
-      const int res = attempt_dp45_mixed<METRIC>(P, S, K, k1_valid, k7_pending, acc, hf);
+      const int res = attempt_dp45_mixed<METRIC>(PL, S, K, k1_valid, k7_pending, acc, hf);
       n_att += 1;
       if (acc) {
         const float4 dx = K.get(kSlotDx);
@@ -298,7 +323,7 @@ __global__ void __launch_bounds__(kTraceBlock, kMixedMinBlocks)
           continue;
         }
         n_acc += 1;
-        const float dr_b = ff_minus(xh_r, K.comp(kSlotXl, 1), P.max_radius_hi, P.max_radius_lo);
+        const float dr_b = ff_minus(xh_r, K.comp(kSlotXl, 1), PL.max_radius_hi, PL.max_radius_lo);
         const bool esc = dr_b <= 0.0f && dr_b + dx.y > 0.0f;
         bool dsk = false;
         if (DISK == kDiskThin) {
@@ -315,7 +340,7 @@ __global__ void __launch_bounds__(kTraceBlock, kMixedMinBlocks)
         }
         mixed_advance(S, K, hf, k1_valid, k7_pending);
       }
-      if (res == kEscaped || n_att >= P.max_steps) {
+      if (res == kEscaped || n_att >= PL.max_steps) {
         pend = kPendFinish | ((uint32_t)(res == kEscaped ? kClsEscaped : kClsMaxSteps)
                               << kPendClsShift);
         live = false;
@@ -333,7 +358,8 @@ __global__ void __launch_bounds__(kTraceBlock, kMixedMinBlocks)
       if (__shfl_sync(kFull, ab, 0)) {
         wdone = true;
         if (live) {
-          mixed_finish(P, O, K, S, kClsBudget, n_att, n_acc, crossed, &bs);
+          mixed_finish(BATCH ? B.scenes[scene].P : P, BATCH ? B.scenes[scene].O : O, K, S,
+                       kClsBudget, n_att, n_acc, crossed, &bs);
           live = false;
         }
       }
@@ -350,9 +376,11 @@ __global__ void __launch_bounds__(kTraceBlock, kMixedMinBlocks)
   }
 }
 
-template <int METRIC, int DISK, bool BUDGET>
+template <int METRIC, int DISK, bool BUDGET, bool BATCH = false, int PERIOD = kPeriod,
+          int MINB = kMixedMinBlocks>
 const void* mixed_fn() {
-  return reinterpret_cast<const void*>(&trace_mixed_kernel<METRIC, DISK, BUDGET>);
+  return reinterpret_cast<const void*>(
+      &trace_mixed_kernel<METRIC, DISK, BUDGET, BATCH, PERIOD, MINB>);
 }
 
 template <bool BUDGET>
@@ -364,23 +392,49 @@ const void* select_mixed_disk(const DevParams& P) {
                              : mixed_fn<kMetricSchwarzschild, kDiskNone, BUDGET>();
 }
 
-const void* select_mixed(const DevParams& P) {
+// Batched launches: the variant (PERIOD, MINB) by index, kBatchVariants of
+// them; the metric and disk kind are the batch's.
+template <int METRIC, int DISK>
+const void* batch_variant(int v) {
+  switch (v) {
+    case 0: return mixed_fn<METRIC, DISK, false, true, 4, 8>();
+    case 1: return mixed_fn<METRIC, DISK, false, true, 2, 8>();
+    case 2: return mixed_fn<METRIC, DISK, false, true, 8, 8>();
+    case 3: return mixed_fn<METRIC, DISK, false, true, 4, 7>();
+    case 4: return mixed_fn<METRIC, DISK, false, true, 2, 7>();
+    default: return mixed_fn<METRIC, DISK, false, true, 8, 7>();
+  }
+}
+
+const void* select_batch(const DevParams& P, int v) {
+  if (P.metric == kMetricKerr)
+    return P.disk == kDiskThin ? batch_variant<kMetricKerr, kDiskThin>(v)
+                               : batch_variant<kMetricKerr, kDiskNone>(v);
+  return P.disk == kDiskThin ? batch_variant<kMetricSchwarzschild, kDiskThin>(v)
+                             : batch_variant<kMetricSchwarzschild, kDiskNone>(v);
+}
+
+const void* select_mixed(const DevParams& P, const BatchTable* batch, int variant) {
+  if (batch) return select_batch(P, variant);
   return P.attempt_budget ? select_mixed_disk<true>(P) : select_mixed_disk<false>(P);
 }
 
 }  // namespace
 
-cudaError_t mixed_occupancy(const DevParams& P, int* blocks_per_sm) {
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, select_mixed(P),
-                                                       kTraceBlock, 0);
+cudaError_t mixed_occupancy(const DevParams& P, int* blocks_per_sm, const BatchTable* batch,
+                            int variant) {
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      blocks_per_sm, select_mixed(P, batch, variant), kTraceBlock, 0);
 }
 
 cudaError_t launch_mixed(const DevParams& P, const DevOutputs& O, DevControl* ctl, int grid,
-                         cudaStream_t stream) {
-  const void* fn = select_mixed(P);
+                         cudaStream_t stream, const BatchTable* batch, int variant) {
+  const void* fn = select_mixed(P, batch, variant);
   DevParams p = P;
   DevOutputs o = O;
-  void* args[] = {&p, &o, &ctl};
+  BatchTable b{};
+  if (batch) b = *batch;
+  void* args[] = {&p, &o, &ctl, &b};
   return cudaLaunchKernel(fn, dim3(grid), dim3(kTraceBlock), args, 0, stream);
 }
 

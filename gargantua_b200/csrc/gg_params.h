@@ -92,8 +92,26 @@ struct QueuedRay {
   double v[4];
   double h;
   double lam;
-  uint64_t idx;  // sample index
+  uint64_t idx;  // sample index (within its scene)
   uint32_t n_att, n_acc;
+  uint32_t scene;  // batched renders: the ray's scene
+  uint32_t pad;
+};
+
+// One scene of a batched render: its parameters (camera, metric, disk, sky,
+// image size; the integrator is the batch's) and its output pointers.
+struct BatchScene {
+  DevParams P;
+  DevOutputs O;
+};
+
+// Where a batched launch finds its scenes: first[k] is the global index of
+// scene k's first sample (first[n] = total samples).
+struct BatchTable {
+  const BatchScene* scenes;
+  const uint64_t* first;
+  uint32_t n;
+  uint32_t pad;
 };
 
 // Device-side counters of one render (reset before each launch).

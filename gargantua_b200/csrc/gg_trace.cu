@@ -25,11 +25,13 @@ namespace {
 // SRC: kSrcCamera traces the render's samples from the camera; kSrcQueue
 // finishes, in FP64, the rays the mixed-precision pass handed over (their
 // count is read from ctl->queued, which that pass wrote before this launch).
-template <int METRIC, int DISK, int STEPPER, int SRC>
+// BATCH (kSrcQueue only): the rays come from a batched render; each carries
+// its scene, whose parameters and outputs are in B.
+template <int METRIC, int DISK, int STEPPER, int SRC, bool BATCH>
 __global__ void __launch_bounds__(kTraceBlock,
                                   METRIC == kMetricKerr ? kTraceMinBlocksKerr : kTraceMinBlocksSchw)
     trace_fp64_kernel(const __grid_constant__ DevParams P, const __grid_constant__ DevOutputs O,
-                      DevControl* ctl) {
+                      DevControl* ctl, const __grid_constant__ BatchTable B) {
   const unsigned lane = threadIdx.x & 31u;
   const uint64_t n_src =
       SRC == kSrcQueue ? (ctl->queued < O.queue_cap ? ctl->queued : O.queue_cap) : P.n_rays;
@@ -40,9 +42,10 @@ __global__ void __launch_bounds__(kTraceBlock,
   if (threadIdx.x < sizeof(BlockStats) / 8)
     reinterpret_cast<unsigned long long*>(&bs)[threadIdx.x] = 0ull;
   __syncthreads();
-  auto finish = [&](uint64_t i, int cls, const Ray& r, uint32_t na, uint32_t nc, double inten_o,
-                    double temp_o, bool cr, double sky_th, double sky_ph) {
-    finish_sample(P, O, i, cls, r, na, nc, inten_o, temp_o, cr, sky_th, sky_ph);
+  auto finish = [&](const DevParams& pp, const DevOutputs& oo, uint64_t i, int cls, const Ray& r,
+                    uint32_t na, uint32_t nc, double inten_o, double temp_o, bool cr,
+                    double sky_th, double sky_ph) {
+    finish_sample(pp, oo, i, cls, r, na, nc, inten_o, temp_o, cr, sky_th, sky_ph);
     atomicAdd(&bs.attempts, (unsigned long long)na);
     atomicAdd(&bs.accepted, (unsigned long long)nc);
     atomicAdd(&bs.cls[cls], 1ull);
@@ -51,6 +54,7 @@ __global__ void __launch_bounds__(kTraceBlock,
 
   Ray R;
   uint64_t idx = 0;
+  uint32_t scene = 0;  // BATCH: the ray's scene
   bool live = false;
   uint32_t n_att = 0, n_acc = 0;
   double inten = 0.0, trans = 1.0;  // volumetric disk accumulators
@@ -107,6 +111,7 @@ __global__ void __launch_bounds__(kTraceBlock,
           R.h = q.h;
           R.lam = q.lam;
           idx = q.idx;
+          if (BATCH) scene = q.scene;
           n_att = n_att0 = q.n_att;
           n_acc = q.n_acc;
         } else {
@@ -132,6 +137,9 @@ __global__ void __launch_bounds__(kTraceBlock,
 #pragma unroll 1
     for (int it = 0; it < kPeriod; ++it) {
       if (!live) continue;
+      // this lane's scene: the batch's entry, or the render's own parameters
+      const DevParams& PL = BATCH ? B.scenes[scene].P : P;
+      const DevOutputs& OL = BATCH ? B.scenes[scene].O : O;
       double xb[4], vb[4];
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
@@ -144,9 +152,9 @@ __global__ void __launch_bounds__(kTraceBlock,
       StepEnd end;
       int res;
       if (STEPPER == kStepperDP45)
-        res = attempt_dp45_fp64<METRIC>(P, R, K, k1_valid, k7_pending, acc, h_used, end);
+        res = attempt_dp45_fp64<METRIC>(PL, R, K, k1_valid, k7_pending, acc, h_used, end);
       else
-        res = attempt_fp64<METRIC>(P, R, K, k1_valid, acc, h_used);
+        res = attempt_fp64<METRIC>(PL, R, K, k1_valid, acc, h_used);
       n_att += 1;
       if (acc) n_acc += 1;
       int done_cls = -1;
@@ -165,8 +173,8 @@ __global__ void __launch_bounds__(kTraceBlock,
 #pragma unroll
         for (int i = 0; i < 4; ++i)
           raw[i] = STEPPER == kStepperDP45 ? end.xraw[i] : xb[i] + h_used * vb[i];
-        const bool esc = (O.cross || (kSkyCross && P.sky == kSkyChecker)) &&
-                         xb[1] <= P.max_radius && raw[1] > P.max_radius;
+        const bool esc = (OL.cross || (kSkyCross && PL.sky == kSkyChecker)) &&
+                         xb[1] <= PL.max_radius && raw[1] > PL.max_radius;
         double d_b = 0.0, d_a = 0.0;
         bool dsk = false;
         if (DISK == kDiskThin) {
@@ -202,12 +210,12 @@ __global__ void __launch_bounds__(kTraceBlock,
           };
           if (esc) {
             double c[8];
-            cross_at(1, P.max_radius, (P.max_radius - xb[1]) / (raw[1] - xb[1]), c);
-            if (O.cross) {
-              store_cross(P, O, idx, c);
+            cross_at(1, PL.max_radius, (PL.max_radius - xb[1]) / (raw[1] - xb[1]), c);
+            if (OL.cross) {
+              store_cross(PL, OL, idx, c);
               crossed = true;
             }
-            if (kSkyCross && P.sky == kSkyChecker) {
+            if (kSkyCross && PL.sky == kSkyChecker) {
               sky_at_cross = true;
               sky_th = c[2];
               sky_ph = c[3];
@@ -218,13 +226,13 @@ __global__ void __launch_bounds__(kTraceBlock,
             const double s = cross_at(2, kHalfPi, d_b / (d_b - d_a), c);
             const double r_c =
                 STEPPER == kStepperDP45 ? c[1] : xb[1] + s * (raw[1] - xb[1]);
-            if (r_c >= P.r_inner && r_c <= P.r_outer) {
+            if (r_c >= PL.r_inner && r_c <= PL.r_outer) {
               c[1] = r_c;
               c[2] = kHalfPi;
-              const double g = redshift_factor<METRIC>(P, r_c, kHalfPi, c + 4);
-              const double q = P.r_inner / r_c;
+              const double g = redshift_factor<METRIC>(PL, r_c, kHalfPi, c + 4);
+              const double q = PL.r_inner / r_c;
               const double g2 = g * g;
-              out_int = (g2 * g2) * pow(q, P.emissivity_index);
+              out_int = (g2 * g2) * pow(q, PL.emissivity_index);
               out_temp = g * pow(q, 0.75);
 #pragma unroll
               for (int i = 0; i < 4; ++i) {
@@ -232,7 +240,7 @@ __global__ void __launch_bounds__(kTraceBlock,
                 R.v[i] = c[4 + i];
               }
               R.lam = lam_b + s * h_used;
-              store_cross(P, O, idx, c);
+              store_cross(PL, OL, idx, c);
               crossed = true;
               done_cls = kClsDisk;
             }
@@ -240,7 +248,7 @@ __global__ void __launch_bounds__(kTraceBlock,
         }
         // Beyond the escape sphere the next attempt only finds r > max_radius
         // and returns Escaped; the ray ends here, counting that attempt.
-        if (sky_at_cross && done_cls < 0 && n_att < P.max_steps) {
+        if (sky_at_cross && done_cls < 0 && n_att < PL.max_steps) {
           n_att += 1;
           done_cls = kClsEscaped;
         }
@@ -256,23 +264,23 @@ __global__ void __launch_bounds__(kTraceBlock,
           sincos(mid[2], &sn, &cs);
           const double cap_r = mid[1] * fabs(sn);
           const double z = mid[1] * cs;
-          if (!(cap_r < P.r_inner || cap_r > P.r_outer)) {
-            const double qq = P.r_inner / cap_r;
-            const double rho = P.density_0 * (qq * qq) *
-                               exp(-z * z / (2.0 * P.scale_height * P.scale_height));
+          if (!(cap_r < PL.r_inner || cap_r > PL.r_outer)) {
+            const double qq = PL.r_inner / cap_r;
+            const double rho = PL.density_0 * (qq * qq) *
+                               exp(-z * z / (2.0 * PL.scale_height * PL.scale_height));
             if (rho > 0.0) {
               const double j = rho * rho * pow(qq, 0.75);
               double pm[4];
 #pragma unroll
               for (int i = 0; i < 4; ++i) pm[i] = 0.5 * (vb[i] + R.v[i]);
-              const double g = redshift_factor<METRIC>(P, mid[1], mid[2], pm);
+              const double g = redshift_factor<METRIC>(PL, mid[1], mid[2], pm);
               const double g2 = g * g;
               inten = inten + j * (g2 * g2) * dlambda * trans;
               trans = trans * exp(-rho * dlambda * 0.1);
               if (trans < 1e-3) {
                 done_cls = kClsDisk;
                 out_int = inten;
-                out_temp = P.temperature_0;
+                out_temp = PL.temperature_0;
               }
             }
           }
@@ -281,16 +289,16 @@ __global__ void __launch_bounds__(kTraceBlock,
           if (inten > 0.0) {
             done_cls = kClsDisk;
             out_int = inten;
-            out_temp = P.temperature_0;
+            out_temp = PL.temperature_0;
           } else {
             done_cls = res == kEscaped ? kClsEscaped : kClsHorizon;
           }
         }
-        if (done_cls < 0 && n_att >= P.max_steps) {
+        if (done_cls < 0 && n_att >= PL.max_steps) {
           if (inten > 0.0) {
             done_cls = kClsDisk;
             out_int = inten;
-            out_temp = P.temperature_0;
+            out_temp = PL.temperature_0;
           } else {
             done_cls = kClsMaxSteps;
           }
@@ -298,10 +306,10 @@ __global__ void __launch_bounds__(kTraceBlock,
       } else if (done_cls < 0) {
         if (res == kHorizon) done_cls = kClsHorizon;
         else if (res == kEscaped) done_cls = kClsEscaped;
-        else if (n_att >= P.max_steps) done_cls = kClsMaxSteps;
+        else if (n_att >= PL.max_steps) done_cls = kClsMaxSteps;
       }
       if (done_cls >= 0) {
-        finish(idx, done_cls, R, n_att, n_acc, out_int, out_temp, crossed,
+        finish(PL, OL, idx, done_cls, R, n_att, n_acc, out_int, out_temp, crossed,
                sky_at_cross ? sky_th : R.x[2], sky_at_cross ? sky_ph : R.x[3]);
         if (SRC == kSrcQueue) atomicAdd(&bs.fp64_att, (unsigned long long)(n_att - n_att0));
         budget_pending += n_att;
@@ -321,7 +329,8 @@ __global__ void __launch_bounds__(kTraceBlock,
       if (__shfl_sync(kFull, ab, 0)) {
         wdone = true;
         if (live) {
-          finish(idx, kClsBudget, R, n_att, n_acc, 0.0, 0.0, crossed, R.x[2], R.x[3]);
+          finish(BATCH ? B.scenes[scene].P : P, BATCH ? B.scenes[scene].O : O, idx, kClsBudget,
+                 R, n_att, n_acc, 0.0, 0.0, crossed, R.x[2], R.x[3]);
           if (SRC == kSrcQueue) atomicAdd(&bs.fp64_att, (unsigned long long)(n_att - n_att0));
           live = false;
         }
@@ -359,9 +368,9 @@ __global__ void reduce_samples_kernel(const __grid_constant__ DevParams P, const
   }
 }
 
-template <int METRIC, int DISK, int STEPPER, int SRC>
+template <int METRIC, int DISK, int STEPPER, int SRC, bool BATCH = false>
 const void* trace_fn() {
-  return reinterpret_cast<const void*>(&trace_fp64_kernel<METRIC, DISK, STEPPER, SRC>);
+  return reinterpret_cast<const void*>(&trace_fp64_kernel<METRIC, DISK, STEPPER, SRC, BATCH>);
 }
 
 template <int STEPPER>
@@ -384,13 +393,19 @@ const void* select_trace(const DevParams& P) {
 }
 
 // The FP64 pass of the mixed form: full Dormand-Prince, thin disk or none.
-const void* select_queue_trace(const DevParams& P) {
+template <bool BATCH>
+const void* select_queue_trace_b(const DevParams& P) {
   if (P.metric == kMetricKerr)
-    return P.disk == kDiskThin ? trace_fn<kMetricKerr, kDiskThin, kStepperDP45, kSrcQueue>()
-                               : trace_fn<kMetricKerr, kDiskNone, kStepperDP45, kSrcQueue>();
+    return P.disk == kDiskThin
+               ? trace_fn<kMetricKerr, kDiskThin, kStepperDP45, kSrcQueue, BATCH>()
+               : trace_fn<kMetricKerr, kDiskNone, kStepperDP45, kSrcQueue, BATCH>();
   return P.disk == kDiskThin
-             ? trace_fn<kMetricSchwarzschild, kDiskThin, kStepperDP45, kSrcQueue>()
-             : trace_fn<kMetricSchwarzschild, kDiskNone, kStepperDP45, kSrcQueue>();
+             ? trace_fn<kMetricSchwarzschild, kDiskThin, kStepperDP45, kSrcQueue, BATCH>()
+             : trace_fn<kMetricSchwarzschild, kDiskNone, kStepperDP45, kSrcQueue, BATCH>();
+}
+
+const void* select_queue_trace(const DevParams& P, bool batch) {
+  return batch ? select_queue_trace_b<true>(P) : select_queue_trace_b<false>(P);
 }
 
 }  // namespace
@@ -401,16 +416,18 @@ cudaError_t trace_occupancy(const DevParams& P, int* blocks_per_sm) {
 }
 
 cudaError_t queue_trace_occupancy(const DevParams& P, int* blocks_per_sm) {
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, select_queue_trace(P),
-                                                       kTraceBlock, 0);
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      blocks_per_sm, select_queue_trace(P, false), kTraceBlock, 0);
 }
 
 cudaError_t launch_queue_trace(const DevParams& P, const DevOutputs& O, DevControl* ctl,
-                               int grid, cudaStream_t stream) {
-  const void* fn = select_queue_trace(P);
+                               int grid, cudaStream_t stream, const BatchTable* batch) {
+  const void* fn = select_queue_trace(P, batch != nullptr);
   DevParams p = P;
   DevOutputs o = O;
-  void* args[] = {&p, &o, &ctl};
+  BatchTable b{};
+  if (batch) b = *batch;
+  void* args[] = {&p, &o, &ctl, &b};
   return cudaLaunchKernel(fn, dim3(grid), dim3(kTraceBlock), args, 0, stream);
 }
 
@@ -419,7 +436,8 @@ cudaError_t launch_trace(const DevParams& P, const DevOutputs& O, DevControl* ct
   const void* fn = select_trace(P);
   DevParams p = P;
   DevOutputs o = O;
-  void* args[] = {&p, &o, &ctl};
+  BatchTable b{};
+  void* args[] = {&p, &o, &ctl, &b};
   return cudaLaunchKernel(fn, dim3(grid), dim3(kTraceBlock), args, 0, stream);
 }
 

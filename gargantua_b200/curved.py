@@ -259,6 +259,57 @@ class Renderer:
                                         C.c_void_p(stream or 0))
         abi.check(st, "gg_render_device")
 
+    # ---- batches ------------------------------------------------------------
+    @staticmethod
+    def _batch_structs(scenes):
+        """gg_scene_t array of `scenes`, and the batch's integrator and options
+        (the first scene's: every scene of a batch shares them)."""
+        arr = (abi.gg_scene_t * len(scenes))()
+        keep = []
+        for k, sc in enumerate(scenes):
+            m, c, d, _, o = sc.c_structs()
+            arr[k].metric = m
+            arr[k].camera = c
+            if d is not None:
+                arr[k].disk = d
+            arr[k].width = sc.width
+            arr[k].height = sc.height
+            arr[k].sky_seed = o.sky_seed
+            keep.append((m, c, d, o))
+        _, _, _, integ, opts = scenes[0].c_structs()
+        return arr, integ, opts, keep
+
+    def render_batch(self, scenes) -> list:
+        """Synchronous batched render (gg_render_batch): one image per scene."""
+        arr, integ, opts, _ = self._batch_structs(scenes)
+        imgs = [np.zeros((sc.height, sc.width, 3), np.uint8) for sc in scenes]
+        ptrs = (C.c_void_p * len(scenes))(*[im.ctypes.data for im in imgs])
+        abi.check(self._lib.gg_render_batch(self._h, arr, len(scenes), C.byref(integ),
+                                            C.byref(opts), ptrs), "gg_render_batch")
+        return imgs
+
+    def render_batch_device(self, scenes, rgb_dev: int, stream: int | None = None) -> None:
+        """Enqueue a batched render writing the concatenated images to rgb_dev."""
+        arr, integ, opts, _ = self._batch_structs(scenes)
+        abi.check(self._lib.gg_render_batch_device(self._h, arr, len(scenes), C.byref(integ),
+                                                   C.byref(opts), C.c_void_p(rgb_dev),
+                                                   C.c_void_p(stream or 0)),
+                  "gg_render_batch_device")
+
+    def batch_autotune(self, scenes):
+        """Times the batch kernel variants on `scenes`, keeps the fastest for
+        this context; returns (variant, per-variant ms)."""
+        arr, integ, opts, _ = self._batch_structs(scenes)
+        v = C.c_int(-1)
+        ms = (C.c_double * abi.GG_BATCH_VARIANTS)()
+        abi.check(self._lib.gg_batch_autotune(self._h, arr, len(scenes), C.byref(integ),
+                                              C.byref(opts), C.byref(v), ms),
+                  "gg_batch_autotune")
+        return v.value, list(ms)
+
+    def batch_set_variant(self, variant: int) -> None:
+        abi.check(self._lib.gg_batch_set_variant(self._h, int(variant)), "gg_batch_set_variant")
+
     def stats(self) -> abi.gg_stats_t:
         s = abi.gg_stats_t()
         abi.check(self._lib.gg_last_stats(self._h, C.byref(s)), "gg_last_stats")

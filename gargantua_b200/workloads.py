@@ -65,3 +65,45 @@ def kerr_stress_4k(precision: int = abi.GG_PREC_FP64, side: int = 4096, spp: int
                  RenderOptions(sky=CheckerSky(18, 36, 0), jitter_spp=spp, seed=1,
                                max_steps=50000, integrator=disk_integrator(stepper),
                                precision=precision))
+
+
+def _splitmix64(x: int) -> tuple[int, int]:
+    """One SplitMix64 step: (new state, output)."""
+    m = (1 << 64) - 1
+    x = (x + 0x9E3779B97F4A7C15) & m
+    z = x
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & m
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & m
+    return x, z ^ (z >> 31)
+
+
+def batch_scenes(n: int = 2048, seed: int = 0, max_side: int = 512,
+                 precision: int = abi.GG_PREC_MIXED) -> list:
+    """n independent Kerr scenes of uneven size for one batched render:
+    spin a ~ U[0, 0.998], camera r ~ U[10, 100] M, inclination ~ U[5, 89] deg,
+    image side ~ U{64, 128, ..., max_side}, thin disk r_ISCO .. r_out with
+    r_out ~ U[15, 40] M, sky seed = scene index; SplitMix64 draws from the
+    master seed.  All share the full Dormand-Prince integrator (rtol 1e-8,
+    atol 1e-10, escape at 200 M) with up to 20,000 step() calls per ray."""
+    state = seed
+    scenes = []
+    sides = max_side // 64
+
+    def uniform():
+        nonlocal state
+        state, z = _splitmix64(state)
+        return (z >> 11) * (1.0 / (1 << 53))
+
+    for k in range(n):
+        spin = 0.998 * uniform()
+        r_cam = 10.0 + 90.0 * uniform()
+        incl = math.radians(5.0 + 84.0 * uniform())
+        side = 64 * (1 + min(sides - 1, int(uniform() * sides)))
+        r_out = 15.0 + 25.0 * uniform()
+        kerr = Kerr(1.0, spin)
+        scenes.append(Scene(kerr, Camera.inclined(r_cam, incl, math.radians(60.0), 1.0), side, side,
+                            ThinDisk(kerr.isco(), r_out, 3.0),
+                            RenderOptions(sky=CheckerSky(18, 36, k), max_steps=20000,
+                                          integrator=disk_integrator(abi.GG_STEPPER_DP45),
+                                          precision=precision)))
+    return scenes

@@ -256,6 +256,50 @@ GG_API int gg_render_device_noalloc(const gg_metric_t* metric, const gg_camera_t
                                     uint32_t height, uint8_t* rgb_dev,
                                     const gg_ray_out_t* rays_dev, void* stream);
 
+/* ---- batched rendering (no reference counterpart) ---------------------- */
+/* One scene of a batch: its own metric, camera, disk, image size and sky
+ * seed.  The integrator and render options are the batch's. */
+typedef struct gg_scene_t {
+  gg_metric_t metric;
+  gg_camera_t camera;
+  gg_disk_t disk;    /* GG_DISK_NONE or GG_DISK_THIN, one kind per batch     */
+  uint32_t width;
+  uint32_t height;
+  uint64_t sky_seed; /* checkerboard seed of this scene                      */
+} gg_scene_t;
+
+#define GG_BATCH_VARIANTS 6 /* kernel variants the batch autotuner chooses from */
+
+/* Renders n scenes in one persistent launch of the mixed-precision kernel
+ * (integ: GG_PREC_MIXED, GG_STEPPER_DP45; opts: one sample per pixel), its
+ * FP64 band pass after it.  All scenes share one metric kind and one disk
+ * kind.  The launch sequence is captured in a CUDA graph per batch shape
+ * (scene count, total samples, integrator and options) and replayed; the
+ * scenes' parameters are uploaded from the context's pinned buffer by a copy
+ * node inside the graph, so a batch of the same shape with new cameras,
+ * spins or disks reuses the graph.  The kernel variant (compaction period x
+ * register budget) is the one gg_batch_autotune chose on this context, or a
+ * fixed default.
+ * gg_render_batch_device: images concatenated in scene order into rgb_dev
+ * (scene k at byte 3 * sum_{j<k} w_j h_j), enqueued on `stream` (NULL = CUDA's
+ * default stream).  gg_render_batch: synchronous, rgb_out[k] = scene k's
+ * host buffer of w_k * h_k * 3 bytes.  Statistics via gg_last_stats. */
+GG_API int gg_render_batch_device(gg_ctx* ctx, const gg_scene_t* scenes, uint32_t n,
+                                  const gg_integrator_t* integ, const gg_render_opts_t* opts,
+                                  uint8_t* rgb_dev, void* stream);
+GG_API int gg_render_batch(gg_ctx* ctx, const gg_scene_t* scenes, uint32_t n,
+                           const gg_integrator_t* integ, const gg_render_opts_t* opts,
+                           uint8_t* const* rgb_out);
+/* Times each of the GG_BATCH_VARIANTS kernel variants on this batch (one
+ * render each, images discarded), keeps the fastest for the context's later
+ * batches and returns its index; ms_out (nullable, GG_BATCH_VARIANTS entries)
+ * receives each variant's device time. */
+GG_API int gg_batch_autotune(gg_ctx* ctx, const gg_scene_t* scenes, uint32_t n,
+                             const gg_integrator_t* integ, const gg_render_opts_t* opts,
+                             int* variant_out, double* ms_out);
+/* Sets the context's batch kernel variant (0 .. GG_BATCH_VARIANTS-1). */
+GG_API int gg_batch_set_variant(gg_ctx* ctx, int variant);
+
 /* ---- measurement ------------------------------------------------------- */
 /* FMA throughput of the context's device in FLOP/s (an FMA counts 2), best
  * of 5 timed launches of independent FMA chains: fp64 = 1 for the FP64 pipe,

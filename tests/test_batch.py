@@ -1,0 +1,99 @@
+"""Batched rendering (gg_render_batch): many scenes of uneven size in one
+persistent launch of the mixed-precision kernel, replayed from a CUDA graph,
+with an autotuned kernel variant.
+
+A batched scene is traced with the same per-ray arithmetic as the scene on
+its own (its parameters are the same numbers; only which warp runs which ray
+differs), so its image must equal the single-scene render byte for byte.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+from gargantua_b200 import abi, workloads
+from gargantua_b200.gr_core import Kerr
+
+
+def test_batch_scene_generator_ranges_and_determinism():
+    a = workloads.batch_scenes(64, seed=0)
+    b = workloads.batch_scenes(64, seed=0)
+    assert [(s.width, s.metric.spin, s.camera.position[1]) for s in a] == \
+        [(s.width, s.metric.spin, s.camera.position[1]) for s in b]
+    for k, s in enumerate(a):
+        assert 0.0 <= s.metric.spin <= 0.998
+        assert 10.0 <= s.camera.position[1] <= 100.0
+        assert math.radians(5.0) <= s.camera.position[2] <= math.radians(89.0)
+        assert s.width == s.height and s.width % 64 == 0 and 64 <= s.width <= 512
+        assert 15.0 <= s.disk.r_outer <= 40.0
+        assert s.options.sky.seed == k
+    assert workloads.batch_scenes(4, seed=1)[0].metric.spin != a[0].metric.spin
+
+
+def _small_batch(n=6):
+    return workloads.batch_scenes(n, seed=3, max_side=128)
+
+
+@pytest.mark.gpu
+def test_batch_equals_single_scene_renders(renderer):
+    scenes = _small_batch()
+    imgs = renderer.render_batch(scenes)
+    st = renderer.stats()
+    assert st.rays == sum(s.n_samples for s in scenes)
+    attempts = 0
+    for sc, img in zip(scenes, imgs):
+        ref, _ = renderer.render(sc)
+        attempts += renderer.stats().attempts
+        assert np.array_equal(img, ref)
+    assert st.attempts == attempts
+
+
+@pytest.mark.gpu
+def test_batch_graph_replay_with_new_parameters(renderer):
+    scenes = _small_batch()
+    first = renderer.render_batch(scenes)
+    again = renderer.render_batch(scenes)  # replays the cached graph
+    assert all(np.array_equal(x, y) for x, y in zip(first, again))
+    # same shape, new spin and camera distance: the graph is reused, the
+    # scene table it uploads is new
+    scenes[2].metric = Kerr(1.0, 0.5)
+    scenes[2].camera.position = (0.0, 33.0, scenes[2].camera.position[2], 0.0)
+    changed = renderer.render_batch(scenes)
+    ref, _ = renderer.render(scenes[2])
+    assert np.array_equal(changed[2], ref)
+    assert not np.array_equal(changed[2], first[2])
+    assert np.array_equal(changed[0], first[0])
+
+
+@pytest.mark.gpu
+def test_batch_autotune_variants_agree(renderer):
+    scenes = _small_batch(4)
+    best, ms = renderer.batch_autotune(scenes)
+    assert 0 <= best < abi.GG_BATCH_VARIANTS
+    assert all(m > 0 for m in ms) and ms[best] == min(ms)
+    outs = []
+    for v in range(abi.GG_BATCH_VARIANTS):
+        renderer.batch_set_variant(v)
+        outs.append(renderer.render_batch(scenes))
+    for o in outs[1:]:
+        assert all(np.array_equal(x, y) for x, y in zip(o, outs[0]))
+    renderer.batch_set_variant(best)
+
+
+@pytest.mark.gpu
+def test_batch_rejects_unsupported(renderer):
+    scenes = _small_batch(3)
+    fp64 = workloads.batch_scenes(3, seed=3, max_side=128, precision=abi.GG_PREC_FP64)
+    with pytest.raises(abi.GargantuaError) as e:
+        renderer.render_batch(fp64)
+    assert e.value.status == abi.GG_ERR_UNSUPPORTED
+    mixed_kinds = scenes[:2] + [workloads.schwarzschild_thin_256(
+        precision=abi.GG_PREC_MIXED, stepper=abi.GG_STEPPER_DP45)]
+    with pytest.raises(abi.GargantuaError) as e:
+        renderer.render_batch(mixed_kinds)
+    assert e.value.status == abi.GG_ERR_UNSUPPORTED
+    # the context stays usable
+    imgs = renderer.render_batch(scenes)
+    assert len(imgs) == 3
