@@ -467,7 +467,7 @@ def run_batch(args) -> None:
             "class_count": [int(x) for x in st.class_count],
             "fp64_band_rays": int(st.fp64_rays), "fp64_band_attempts": int(st.fp64_attempts),
             "autotune": {"variant": variant, "variant_ms_on_every_8th_scene": tune_ms,
-                         "variants": "0..5 = (period, CTAs/SM) (4,8) (2,8) (8,8) (4,7) (2,7) (8,7)",
+                         "variants": "0..5 = (period, CTAs/SM) (16,8) (8,8) (4,8) (16,7) (8,7) (4,7)",
                          "wall_s": tune_s},
             "one_launch_per_scene": {"ms": single_ms, "geodesics_per_s": n / (single_ms * 1e-3)},
             "batch_over_one_launch_per_scene": single_ms / best}

@@ -1,7 +1,7 @@
 // gg_mixed.cu -- the mixed-precision persistent trace kernel (GG_PREC_MIXED).
 //
 // Same work decomposition as the FP64 kernel (gg_trace.cu): persistent CTAs,
-// 32-sample chunks per warp, ballot refill every kPeriod attempts.  Each lane
+// 32-sample chunks per warp, ballot refill every PERIOD attempts.  Each lane
 // steps its ray with the mixed-precision full Dormand-Prince attempt
 // (gg_mixed.cuh).  When a ray's next attempt would start inside the FP64
 // band -- r within 0.5 M of the horizon (with its buffer) or of the prograde
@@ -294,7 +294,7 @@ __global__ void __launch_bounds__(kTraceBlock, MINB)
     }
     if (!__any_sync(kFull, live)) break;
 
-    // ---- advance every live ray by up to kPeriod attempts -----------------
+    // ---- advance every live ray by up to PERIOD attempts ------------------
 #pragma unroll 1
     for (int it = 0; it < PERIOD; ++it) {
       if (!live) continue;
@@ -376,7 +376,7 @@ __global__ void __launch_bounds__(kTraceBlock, MINB)
   }
 }
 
-template <int METRIC, int DISK, bool BUDGET, bool BATCH = false, int PERIOD = kPeriod,
+template <int METRIC, int DISK, bool BUDGET, bool BATCH = false, int PERIOD = kMixedPeriod,
           int MINB = kMixedMinBlocks>
 const void* mixed_fn() {
   return reinterpret_cast<const void*>(
@@ -397,12 +397,12 @@ const void* select_mixed_disk(const DevParams& P) {
 template <int METRIC, int DISK>
 const void* batch_variant(int v) {
   switch (v) {
-    case 0: return mixed_fn<METRIC, DISK, false, true, 4, 8>();
-    case 1: return mixed_fn<METRIC, DISK, false, true, 2, 8>();
-    case 2: return mixed_fn<METRIC, DISK, false, true, 8, 8>();
-    case 3: return mixed_fn<METRIC, DISK, false, true, 4, 7>();
-    case 4: return mixed_fn<METRIC, DISK, false, true, 2, 7>();
-    default: return mixed_fn<METRIC, DISK, false, true, 8, 7>();
+    case 0: return mixed_fn<METRIC, DISK, false, true, 16, 8>();
+    case 1: return mixed_fn<METRIC, DISK, false, true, 8, 8>();
+    case 2: return mixed_fn<METRIC, DISK, false, true, 4, 8>();
+    case 3: return mixed_fn<METRIC, DISK, false, true, 16, 7>();
+    case 4: return mixed_fn<METRIC, DISK, false, true, 8, 7>();
+    default: return mixed_fn<METRIC, DISK, false, true, 4, 7>();
   }
 }
 

@@ -16,10 +16,19 @@ namespace gg {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
+// Attempts between refills: the FP64 kernel's and the mixed kernel's
+// (single-scene renders; batches autotune theirs).  Measured on the 1080p
+// Kerr frame, FP64 drop-in / mixed ms: period 2: 52.9 / 33.4, 4: 49.9 / 31.1,
+// 8: 47.0 / 29.3, 16: 45.3 / 29.2, 32: 44.3 / 29.4 (fewer ballots and
+// refills; lanes that finish early wait longer).
 #ifndef GG_TRACE_PERIOD
-#define GG_TRACE_PERIOD 4
+#define GG_TRACE_PERIOD 32
 #endif
-constexpr int kPeriod = GG_TRACE_PERIOD;  // attempts between refills
+#ifndef GG_MIXED_PERIOD
+#define GG_MIXED_PERIOD 16
+#endif
+constexpr int kPeriod = GG_TRACE_PERIOD;
+constexpr int kMixedPeriod = GG_MIXED_PERIOD;
 constexpr uint32_t kChunk = 32;  // samples a warp takes from the queue at once
 
 GG_DEV unsigned lanemask_lt() {
