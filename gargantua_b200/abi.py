@@ -145,6 +145,11 @@ _SIGNATURES = {
     "gg_batch_autotune": (C.c_int, [C.c_void_p, P(gg_scene_t), C.c_uint32, P(gg_integrator_t),
                                     P(gg_render_opts_t), P(C.c_int), P(C.c_double)]),
     "gg_batch_set_variant": (C.c_int, [C.c_void_p, C.c_int]),
+    "gg_forward_ckpt": (C.c_int, [C.c_void_p, P(gg_metric_t), C.c_double, C.c_double, C.c_double,
+                                  C.c_double, P(gg_disk_t), P(gg_integrator_t),
+                                  P(gg_render_opts_t), C.c_uint32, C.c_uint32, C.c_void_p,
+                                  C.c_void_p]),
+    "gg_backward": (C.c_int, [C.c_void_p, C.c_void_p, P(C.c_double), C.c_void_p]),
     "gg_render_device_noalloc": (C.c_int, [P(gg_metric_t), P(gg_camera_t), P(gg_disk_t),
                                            P(gg_integrator_t), P(gg_render_opts_t), C.c_uint32,
                                            C.c_uint32, C.c_void_p, P(gg_ray_out_t),

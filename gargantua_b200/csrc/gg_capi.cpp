@@ -53,6 +53,16 @@ struct gg_ctx {
     int metric = -1, disk = -1;
   } batch_key;
   cudaGraphExec_t batch_exec = nullptr;
+  // differentiable render: the last forward's parameters and per-ray records
+  DevParams diff_P{};
+  bool diff_ready = false;
+  uint32_t diff_ckpt_per_ray = 0;
+  void* diff_rays = nullptr;
+  size_t diff_rays_cap = 0;
+  void* diff_ckpt = nullptr;
+  size_t diff_ckpt_cap = 0;
+  double* diff_grad = nullptr;       // 5 doubles, device
+  double* diff_grad_host = nullptr;  // pinned
   bool pending = false;            // stats of the last device-pointer render not read yet
   gg_stats_t last{};
   std::mutex mu;
@@ -775,6 +785,10 @@ GG_API int gg_destroy(gg_ctx* c) {
   if (c->batch_exec) cudaGraphExecDestroy(c->batch_exec);
   if (c->batch_dev) cudaFree(c->batch_dev);
   if (c->batch_host) cudaFreeHost(c->batch_host);
+  if (c->diff_rays) cudaFree(c->diff_rays);
+  if (c->diff_ckpt) cudaFree(c->diff_ckpt);
+  if (c->diff_grad) cudaFree(c->diff_grad);
+  if (c->diff_grad_host) cudaFreeHost(c->diff_grad_host);
   if (c->ctl) cudaFree(c->ctl);
   if (c->ctl_host) cudaFreeHost(c->ctl_host);
   if (c->ev_start) cudaEventDestroy(c->ev_start);
@@ -911,6 +925,75 @@ GG_API int gg_batch_set_variant(gg_ctx* c, int variant) {
   if (!c || variant < 0 || variant >= GG_BATCH_VARIANTS) return GG_ERR_INVALID_ARG;
   Lock lock(c);
   c->batch_variant = variant;
+  return GG_OK;
+}
+
+GG_API int gg_forward_ckpt(gg_ctx* c, const gg_metric_t* metric, double r_cam,
+                           double inclination, double fov_y_radians, double aspect,
+                           const gg_disk_t* disk, const gg_integrator_t* integ,
+                           const gg_render_opts_t* opts, uint32_t width, uint32_t height,
+                           double* rgb_lin_dev, void* stream) {
+  if (!c || !metric || !disk || !integ || !opts || !rgb_lin_dev) return GG_ERR_INVALID_ARG;
+  gg_camera_t cam;
+  if (gg_camera_inclined(&cam, r_cam, inclination, fov_y_radians, aspect) != GG_OK)
+    return GG_ERR_INVALID_ARG;
+  const int v = validate(metric, &cam, disk, integ, opts, width, height);
+  if (v != GG_OK) return v;
+  if (metric->kind != GG_METRIC_KERR || disk->kind != GG_DISK_THIN ||
+      integ->precision != GG_PREC_FP64 || integ->stepper != GG_STEPPER_DP45 ||
+      opts->samples_per_axis > 1 || opts->jitter_spp > 0 || opts->attempt_budget != 0)
+    return GG_ERR_UNSUPPORTED;
+  Lock lock(c);
+  DevParams P;
+  build_params(metric, &cam, disk, integ, opts, width, height, &P);
+  const uint32_t cpr = integ->max_steps / 32 + 2;
+  int st = grow(&c->diff_rays, &c->diff_rays_cap, sizeof(gg::DiffRay) * P.n_rays);
+  if (st != GG_OK) return st;
+  st = grow(&c->diff_ckpt, &c->diff_ckpt_cap, sizeof(gg::Ckpt) * cpr * P.n_rays);
+  if (st != GG_OK) return st;
+  gg::DiffOut D{static_cast<gg::DiffRay*>(c->diff_rays), static_cast<gg::Ckpt*>(c->diff_ckpt),
+                cpr, 0u, rgb_lin_dev};
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (cudaStreamWaitEvent(s, c->ev_done, 0) != cudaSuccess) return GG_ERR_CUDA;
+  if (cudaEventRecord(c->ev_start, s) != cudaSuccess) return GG_ERR_CUDA;
+  if (gg::launch_diff_forward(P, D, c->sms, s) != cudaSuccess) return GG_ERR_CUDA;
+  if (cudaEventRecord(c->ev_stop, s) != cudaSuccess) return GG_ERR_CUDA;
+  if (cudaEventRecord(c->ev_done, s) != cudaSuccess) return GG_ERR_CUDA;
+  c->diff_P = P;
+  c->diff_ckpt_per_ray = cpr;
+  c->diff_ready = true;
+  return GG_OK;
+}
+
+GG_API int gg_backward(gg_ctx* c, const double* dl_drgb_dev, double grad[5], void* stream) {
+  if (!c || !dl_drgb_dev || !grad) return GG_ERR_INVALID_ARG;
+  Lock lock(c);
+  if (!c->diff_ready) return GG_ERR_INVALID_ARG;
+  if (!c->diff_grad && cudaMalloc(&c->diff_grad, 5 * sizeof(double)) != cudaSuccess) {
+    cudaGetLastError();
+    c->diff_grad = nullptr;
+    return GG_ERR_OOM;
+  }
+  if (!c->diff_grad_host &&
+      cudaMallocHost(&c->diff_grad_host, 5 * sizeof(double)) != cudaSuccess) {
+    cudaGetLastError();
+    c->diff_grad_host = nullptr;
+    return GG_ERR_OOM;
+  }
+  gg::DiffOut D{static_cast<gg::DiffRay*>(c->diff_rays), static_cast<gg::Ckpt*>(c->diff_ckpt),
+                c->diff_ckpt_per_ray, 0u, nullptr};
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (cudaStreamWaitEvent(s, c->ev_done, 0) != cudaSuccess) return GG_ERR_CUDA;
+  if (cudaMemsetAsync(c->diff_grad, 0, 5 * sizeof(double), s) != cudaSuccess) return GG_ERR_CUDA;
+  if (gg::launch_diff_backward(c->diff_P, D, dl_drgb_dev, c->diff_grad, c->sms, s) !=
+      cudaSuccess)
+    return GG_ERR_CUDA;
+  if (cudaMemcpyAsync(c->diff_grad_host, c->diff_grad, 5 * sizeof(double),
+                      cudaMemcpyDeviceToHost, s) != cudaSuccess)
+    return GG_ERR_CUDA;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return GG_ERR_CUDA;
+  for (int i = 0; i < 5; ++i) grad[i] = c->diff_grad_host[i];
+  cudaEventRecord(c->ev_done, s);
   return GG_OK;
 }
 

@@ -354,6 +354,12 @@ struct KStore {
   GG_DEV double& operator()(int stage, int i) const { return s[stage][i][threadIdx.x]; }
 };
 
+// The same store in a per-thread array (local memory).
+struct KStoreLocal {
+  double (*k)[4];  // [7][4]
+  GG_DEV double& operator()(int stage, int i) const { return k[stage][i]; }
+};
+
 // v + h (c1 k1 + c3 k3 + c4 k4 + c5 k5 + c6 k6), left to right, uncontracted
 // (geodesic.rs:294-295).
 GG_DEV double combine5(double v, double h, double k1, double k3, double k4, double k5,
@@ -612,9 +618,11 @@ struct StepEnd {
 
 // One full Dormand-Prince attempt in FP64.  Same contract as attempt_fp64;
 // with k1_valid the previous step's last stage (K(6, .), evaluated at the
-// accepted state) is copied to K(0, .) first.
-template <int METRIC>
-GG_DEV int attempt_dp45_fp64(const DevParams& P, Ray& R, const KStore& K, bool& k1_valid,
+// accepted state) is copied to K(0, .) first.  KS is where the stage
+// derivatives live: KStore (shared memory) or KStoreLocal (this thread's
+// local memory, for the differentiable render's one-ray-per-thread kernels).
+template <int METRIC, class KS>
+GG_DEV int attempt_dp45_fp64(const DevParams& P, Ray& R, const KS& K, bool& k1_valid,
                              bool& k7_pending, bool& accepted, double& h_used, StepEnd& end) {
   accepted = false;
   if (R.x[1] > P.max_radius) return kEscaped;

@@ -105,6 +105,27 @@ struct BatchScene {
   DevOutputs O;
 };
 
+// Differentiable render (gg_forward_ckpt / gg_backward): what the forward
+// pass keeps per ray for the backward pass.
+struct DiffRay {
+  uint32_t n_acc;   // accepted steps
+  uint32_t n_ckpt;  // checkpoints stored; the first is the initial state
+  int32_t cls;
+  uint32_t pad;
+};
+struct Ckpt {  // state after every kCkptEvery-th accepted step, and the next step size
+  double x[4];
+  double v[4];
+  double h;
+};
+struct DiffOut {
+  DiffRay* rays;
+  Ckpt* ckpt;          // ckpt_per_ray entries per ray
+  uint32_t ckpt_per_ray;
+  uint32_t pad;
+  double* rgb;         // 3 per ray: linear colour (the differentiated image)
+};
+
 // Where a batched launch finds its scenes: first[k] is the global index of
 // scene k's first sample (first[n] = total samples).
 struct BatchTable {

@@ -300,6 +300,27 @@ GG_API int gg_batch_autotune(gg_ctx* ctx, const gg_scene_t* scenes, uint32_t n,
 /* Sets the context's batch kernel variant (0 .. GG_BATCH_VARIANTS-1). */
 GG_API int gg_batch_set_variant(gg_ctx* ctx, int variant);
 
+/* ---- differentiable render (no reference counterpart) ------------------- */
+/* Forward pass of the differentiable render: Kerr (metric), the inclined
+ * camera gg_camera_inclined(r_cam, inclination, fov_y, aspect), a thin disk,
+ * integ GG_PREC_FP64 + GG_STEPPER_DP45, opts one sample per pixel and no
+ * budget.  Writes the linear RGB image (width*height*3 doubles, row-major,
+ * device pointer) on `stream` and keeps, in the context, per-ray
+ * checkpoints of the state every 32 accepted steps for gg_backward.
+ * The image is a function of p = (spin, inclination, r_cam, disk r_inner,
+ * disk emissivity_index). */
+GG_API int gg_forward_ckpt(gg_ctx* ctx, const gg_metric_t* metric, double r_cam,
+                           double inclination, double fov_y_radians, double aspect,
+                           const gg_disk_t* disk, const gg_integrator_t* integ,
+                           const gg_render_opts_t* opts, uint32_t width, uint32_t height,
+                           double* rgb_lin_dev, void* stream);
+/* Adjoint of the last gg_forward_ckpt on this context: given dL/d(image)
+ * (device, same layout), writes dL/dp to grad[5] (host) in the order above.
+ * Disk pixels carry the gradient (through the geodesics, the redshift and
+ * the emissivity); sky and horizon pixels are piecewise constant in p.
+ * Recomputes trajectories from the checkpoints.  Synchronises `stream`. */
+GG_API int gg_backward(gg_ctx* ctx, const double* dl_drgb_dev, double grad[5], void* stream);
+
 /* ---- measurement ------------------------------------------------------- */
 /* FMA throughput of the context's device in FLOP/s (an FMA counts 2), best
  * of 5 timed launches of independent FMA chains: fp64 = 1 for the FP64 pipe,
