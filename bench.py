@@ -11,9 +11,11 @@ is procedural (nothing to load), so "inputs resident" means the parameter
 block only.  Between timed steps a 256 MiB buffer is written to flush L2.
 
 One JSON line on rank 0.  ``value`` is whole-job geodesics/s of the mixed
-FP32/FP64 form (full Dormand-Prince stepper; rays traced to termination per
-second, summed over ranks; each rank renders its own frame: weak scaling, no
-collective on the data path).  ``forms`` times the same frame as the plain
+FP32/FP64 form (full Dormand-Prince stepper; rays of the frame traced to
+termination per second).  With N ranks the one frame is split by interleaved
+rows (rank k traces rows k, k+N, ...; strong scaling), and each step ends
+with the all-gather of every rank's RGB8 rows, the only collective; the
+step time is the max over ranks.  ``forms`` times the same frame as the plain
 FP64 drop-in (the reference's step) and as FP64 with the mixed form's
 stepper; ``mixed_over_fp64`` and ``mixed_over_fp64_dp45`` are the ratios,
 ``endpoint_error`` the mixed form's crossing-state error and class agreement
@@ -136,6 +138,16 @@ def barrier(world):
         dist.barrier()
 
 
+def sum_over_ranks(x: int, world: int) -> int:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.int64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return int(t.item())
+
+
 def max_over_ranks(x: float, world: int) -> float:
     if world == 1:
         return x
@@ -147,9 +159,23 @@ def max_over_ranks(x: float, world: int) -> float:
 
 
 def time_form(r, scene, steps, warmup, world, flush, with_clocks, device_index):
-    """Device-timed renders of `scene` with device-resident outputs."""
+    """Device-timed renders of `scene` (this rank's rows of the frame) with
+    device-resident outputs; with N > 1 ranks each step also gathers every
+    rank's RGB8 rows (NCCL all-gather), the frame's one collective."""
     import torch
-    out = torch.empty(scene.width * scene.height * 3, dtype=torch.uint8, device="cuda")
+    rows = scene.rows
+    out = torch.empty(scene.width * rows * 3, dtype=torch.uint8, device="cuda")
+    gathered = None
+    if world > 1:
+        import torch.distributed as dist
+        max_rows = (scene.height + world - 1) // world
+        pad = torch.zeros(max_rows * scene.width * 3, dtype=torch.uint8, device="cuda")
+        gathered = torch.empty(world * pad.numel(), dtype=torch.uint8, device="cuda")
+
+    def gather():
+        if world > 1:
+            pad[: out.numel()] = out
+            dist.all_gather_into_tensor(gathered, pad)
     # everything (flush, events, renders) on the library context's own stream
     stream = torch.cuda.ExternalStream(r.stream)
     for _ in range(warmup):
@@ -161,10 +187,13 @@ def time_form(r, scene, steps, warmup, world, flush, with_clocks, device_index):
     torch.cuda.synchronize()
     clk = ClockSampler(device_index) if with_clocks else None
     with torch.cuda.stream(stream):
+        for _ in range(warmup if world > 1 else 0):
+            gather()
         for i in range(steps):
             flush.zero_()
             ev[i][0].record(stream)
             r.render_device(scene, out.data_ptr(), None, r.stream)
+            gather()
             ev[i][1].record(stream)
     stream.synchronize()
     torch.cuda.synchronize()
@@ -179,7 +208,7 @@ def time_form(r, scene, steps, warmup, world, flush, with_clocks, device_index):
 def time_e2e(r, scene, steps, warmup, world):
     import numpy as np
     import torch
-    host = torch.empty(scene.width * scene.height * 3, dtype=torch.uint8,
+    host = torch.empty(scene.width * scene.rows * 3, dtype=torch.uint8,
                        pin_memory=True).numpy()
     for _ in range(warmup):
         r.render_into(scene, host)
@@ -217,7 +246,7 @@ def run_ours(args) -> None:
     import numpy as np
     import torch
 
-    from gargantua_b200 import abi, flops, workloads
+    from gargantua_b200 import abi, flops, shard, workloads
     from gargantua_b200.accuracy import crossing_geo_err
     from gargantua_b200.curved import Renderer
 
@@ -239,21 +268,25 @@ def run_ours(args) -> None:
     for form, prec, stepper in (("fp64", abi.GG_PREC_FP64, abi.GG_STEPPER_REFERENCE),
                                 ("fp64_dp45", abi.GG_PREC_FP64, abi.GG_STEPPER_DP45),
                                 ("mixed", abi.GG_PREC_MIXED, abi.GG_STEPPER_DP45)):
-        scene = workloads.kerr_thin_1080p(precision=prec, stepper=stepper)
+        full = workloads.kerr_thin_1080p(precision=prec, stepper=stepper)
+        # N > 1: this rank's interleaved rows of the one frame (strong scaling)
+        scene = shard.shard_scene(full, rank, world) if world > 1 else full
         res = time_form(r, scene, steps, warmup, world, flush, form == "mixed", local)
         st = res["stats"]
         mean_ms = statistics.mean(res["ms"])
+        attempts = sum_over_ranks(int(st.attempts), world)
+        accepted = sum_over_ranks(int(st.accepted), world)
         forms[form] = {
-            "geodesics_per_s": world * scene.n_samples * steps / (res["total_ms"] * 1e-3),
+            "geodesics_per_s": full.n_samples * steps / (res["total_ms"] * 1e-3),
             "ms_per_step": res["total_ms"] / steps,
             "launch_ms_mean": mean_ms,
-            "attempts_per_frame": int(st.attempts),
-            "accepted_per_frame": int(st.accepted),
-            "attempts_per_s": world * st.attempts * steps / (res["total_ms"] * 1e-3),
-            "accepted_steps_per_s": world * st.accepted * steps / (res["total_ms"] * 1e-3),
+            "attempts_per_frame": attempts,
+            "accepted_per_frame": accepted,
+            "attempts_per_s": attempts * steps / (res["total_ms"] * 1e-3),
+            "accepted_steps_per_s": accepted * steps / (res["total_ms"] * 1e-3),
             "class_count": [int(x) for x in st.class_count],
             "fp64_band_rays": int(st.fp64_rays), "fp64_band_attempts": int(st.fp64_attempts),
-            "clocks": res["clocks"], "scene": scene,
+            "clocks": res["clocks"], "scene": scene, "full": full, "stats_attempts": st.attempts,
         }
     head = "mixed"
     H = forms[head]
@@ -266,7 +299,8 @@ def run_ours(args) -> None:
     fp64_peak = r.fma_peak(fp64=True)
     fp32_peak = r.fma_peak(fp64=False)
     peak = fp32_peak
-    achieved = H["attempts_per_frame"] * fpa / (H["launch_ms_mean"] * 1e-3)
+    # this rank's launches (its attempts over its launch time)
+    achieved = int(H["stats_attempts"]) * fpa / (H["launch_ms_mean"] * 1e-3)
 
     # endpoint error of the mixed form against the FP64 kernel of the same
     # method (held to the CPU oracle at 1e-9 by the parity tests): crossing
@@ -292,14 +326,14 @@ def run_ours(args) -> None:
     line = {
         "metric": METRIC, "value": H["geodesics_per_s"], "unit": UNIT, "n_gpus": world,
         "steps": steps, "warmup": warmup, "ms_per_step": H["ms_per_step"],
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
         "dtype": "f32+f64",
         "data": "synthetic: procedural Kerr scene, seeded checkerboard sky",
         "config": workload_config(scene, head),
         "clocks": H["clocks"],
-        "e2e": {"value": world * scene.n_samples * steps / e2e_s, "unit": UNIT,
+        "e2e": {"value": H["full"].n_samples * steps / e2e_s, "unit": UNIT,
                 "h2d_bytes_per_step": abi.load().gg_struct_size(b"launch_params"),
-                "d2h_bytes_per_step": scene.width * scene.height * 3},
+                "d2h_bytes_per_step": scene.width * scene.rows * 3},
         # per step: the mixed kernel and the FP64 band pass
         "gpu_launches": 2 * steps,
         "roofline": {"bound": "fp32", "achieved": achieved / 1e12,
@@ -309,7 +343,8 @@ def run_ours(args) -> None:
                      "flops_per_attempt": fpa,
                      "peak_source": "measured in this run by gg_measure_fma_peak (FMA chains);"
                                     " MEASURED_PEAKS.json has no FP64/FP32 ALU figure"},
-        "forms": {k: {kk: vv for kk, vv in v.items() if kk not in ("scene", "clocks")}
+        "forms": {k: {kk: vv for kk, vv in v.items()
+                      if kk not in ("scene", "clocks", "full", "stats_attempts")}
                   for k, v in forms.items()},
         "fma_peak_tflops": {"fp64": fp64_peak / 1e12, "fp32": fp32_peak / 1e12},
         "attempts_per_ray_pct": {"p50": pct[0], "p90": pct[1], "p99": pct[2], "p99.9": pct[3],

@@ -74,8 +74,8 @@ class gg_integrator_t(C.Structure):
 class gg_render_opts_t(C.Structure):
     _fields_ = [("samples_per_axis", C.c_uint32), ("jitter_spp", C.c_uint32),
                 ("seed", C.c_uint64), ("sky", C.c_int32), ("sky_rows", C.c_uint32),
-                ("sky_cols", C.c_uint32), ("reserved", C.c_uint32), ("sky_seed", C.c_uint64),
-                ("attempt_budget", C.c_uint64)]
+                ("sky_cols", C.c_uint32), ("row_offset", C.c_uint32), ("sky_seed", C.c_uint64),
+                ("attempt_budget", C.c_uint64), ("row_step", C.c_uint32), ("reserved", C.c_uint32)]
 
 
 class gg_ray_out_t(C.Structure):

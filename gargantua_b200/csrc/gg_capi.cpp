@@ -132,6 +132,12 @@ bool finite_all(const double* p, int n) {
   return true;
 }
 
+// Image rows a render traces: row_offset, row_offset + row_step, ...
+uint32_t rows_of(const gg_render_opts_t& o, uint32_t height) {
+  const uint32_t step = o.row_step > 1 ? o.row_step : 1;
+  return o.row_offset >= height ? 0u : (height - o.row_offset + step - 1) / step;
+}
+
 uint32_t spp_of(const gg_render_opts_t& o) {
   if (o.jitter_spp > 0) return o.jitter_spp;
   const uint32_t spa = o.samples_per_axis < 1 ? 1 : o.samples_per_axis;
@@ -196,7 +202,9 @@ int validate(const gg_metric_t* metric, const gg_camera_t* camera, const gg_disk
   const uint64_t spa = opts->samples_per_axis < 1 ? 1 : opts->samples_per_axis;
   if (opts->jitter_spp == 0 && (spa * width > 0xffffffffull || spa * height > 0xffffffffull))
     return GG_ERR_INVALID_ARG;
-  const uint64_t n = (uint64_t)width * height * spp_of(*opts);
+  const uint32_t step = opts->row_step > 1 ? opts->row_step : 1;
+  if (opts->row_offset >= step || opts->row_offset >= height) return GG_ERR_INVALID_ARG;
+  const uint64_t n = (uint64_t)width * rows_of(*opts, height) * spp_of(*opts);
   if (n == 0 || n > (1ull << 40)) return GG_ERR_INVALID_ARG;
   return GG_OK;
 }
@@ -269,7 +277,10 @@ void build_params(const gg_metric_t* metric, const gg_camera_t* camera, const gg
   P.sub_w = width * P.spa;
   P.sub_h = height * P.spa;
   P.seed = opts->seed;
-  P.n_rays = (uint64_t)width * height * P.spp;
+  P.row_step = opts->row_step > 1 ? opts->row_step : 1;
+  P.row0 = opts->row_offset;
+  P.rows = rows_of(*opts, height);
+  P.n_rays = (uint64_t)width * P.rows * P.spp;
   P.inv_spp = 1.0 / (double)P.spp;
 
   // Camera::pixel_direction frame (camera.rs:20-29)
@@ -457,7 +468,8 @@ int batch_prepare(gg_ctx* c, const gg_scene_t* scenes, uint32_t n, const gg_inte
   if (!scenes || n == 0 || !integ || !opts) return GG_ERR_INVALID_ARG;
   if (integ->precision != GG_PREC_MIXED || integ->stepper != GG_STEPPER_DP45)
     return GG_ERR_UNSUPPORTED;
-  if (opts->samples_per_axis > 1 || opts->jitter_spp > 0 || opts->attempt_budget != 0)
+  if (opts->samples_per_axis > 1 || opts->jitter_spp > 0 || opts->attempt_budget != 0 ||
+      opts->row_step > 1)
     return GG_ERR_UNSUPPORTED;
   const int kind = scenes[0].metric.kind, disk_kind = scenes[0].disk.kind;
   if (disk_kind != GG_DISK_NONE && disk_kind != GG_DISK_THIN) return GG_ERR_UNSUPPORTED;
@@ -941,7 +953,8 @@ GG_API int gg_forward_ckpt(gg_ctx* c, const gg_metric_t* metric, double r_cam,
   if (v != GG_OK) return v;
   if (metric->kind != GG_METRIC_KERR || disk->kind != GG_DISK_THIN ||
       integ->precision != GG_PREC_FP64 || integ->stepper != GG_STEPPER_DP45 ||
-      opts->samples_per_axis > 1 || opts->jitter_spp > 0 || opts->attempt_budget != 0)
+      opts->samples_per_axis > 1 || opts->jitter_spp > 0 || opts->attempt_budget != 0 ||
+      opts->row_step > 1)
     return GG_ERR_UNSUPPORTED;
   Lock lock(c);
   DevParams P;
@@ -1010,7 +1023,7 @@ GG_API int gg_render(gg_ctx* c, const gg_metric_t* metric, const gg_camera_t* ca
   build_params(metric, camera, disk, integ, opts, width, height, &P);
   Lock lock(c);
   const uint64_t n = P.n_rays;
-  const size_t n_pix = (size_t)width * height;
+  const size_t n_pix = (size_t)width * P.rows;
 
   // lay out the device staging buffer for every requested output
   struct Slot {

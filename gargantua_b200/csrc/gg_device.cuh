@@ -832,11 +832,15 @@ GG_DEV double jitter_unit(uint64_t seed, uint64_t key) {
 GG_DEV void sample_uv(const DevParams& P, uint64_t idx, double& u, double& v) {
   const uint64_t pix = idx / P.spp;
   const uint32_t s = (uint32_t)(idx - pix * P.spp);
-  const uint32_t py = (uint32_t)(pix / P.width);
-  const uint32_t px = (uint32_t)(pix - (uint64_t)py * P.width);
+  const uint32_t prow = (uint32_t)(pix / P.width);  // row among the traced rows
+  const uint32_t px = (uint32_t)(pix - (uint64_t)prow * P.width);
+  const uint32_t py = P.row0 + prow * P.row_step;   // row of the image
   if (P.jitter_spp > 0) {
-    const double ox = jitter_unit(P.seed, 2 * idx);
-    const double oy = jitter_unit(P.seed, 2 * idx + 1);
+    // keyed by the sample's index in the whole image, so a frame split
+    // across GPUs jitters every sample as the unsplit frame does
+    const uint64_t gidx = ((uint64_t)py * P.width + px) * P.spp + s;
+    const double ox = jitter_unit(P.seed, 2 * gidx);
+    const double oy = jitter_unit(P.seed, 2 * gidx + 1);
     u = sub_rn(mul_rn(__ddiv_rn(add_rn((double)px, ox), (double)P.width), 2.0), 1.0);
     v = sub_rn(1.0, mul_rn(__ddiv_rn(add_rn((double)py, oy), (double)P.height), 2.0));
     return;

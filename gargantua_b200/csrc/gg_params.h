@@ -42,6 +42,8 @@ struct DevParams {
   // sampling
   uint32_t width, height, spa, spp, jitter_spp, sub_w, sub_h;
   uint32_t pad0;
+  uint32_t row0, row_step, rows;  // traced rows: row0 + k row_step, k < rows
+  uint32_t pad_rows;
   uint64_t seed;
   uint64_t n_rays;
   // camera frame (camera.rs:20-29, ray.rs:29-48), host-evaluated

@@ -354,7 +354,7 @@ __global__ void __launch_bounds__(kTraceBlock,
 // encodes sRGB (render_row, renderer.rs:326-343).
 __global__ void reduce_samples_kernel(const __grid_constant__ DevParams P, const double* samples,
                                       uint8_t* rgb8) {
-  const uint64_t n_pix = (uint64_t)P.width * P.height;
+  const uint64_t n_pix = (uint64_t)P.width * P.rows;
   for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n_pix;
        p += (uint64_t)gridDim.x * blockDim.x) {
     double acc[3] = {0.0, 0.0, 0.0};
@@ -443,7 +443,7 @@ cudaError_t launch_trace(const DevParams& P, const DevOutputs& O, DevControl* ct
 
 cudaError_t launch_reduce(const DevParams& P, const double* samples, uint8_t* rgb8, int sms,
                           cudaStream_t stream) {
-  const uint64_t n_pix = (uint64_t)P.width * P.height;
+  const uint64_t n_pix = (uint64_t)P.width * P.rows;
   uint64_t blocks = (n_pix + 255) / 256;
   const uint64_t cap = (uint64_t)sms * 8;
   if (blocks > cap) blocks = cap;

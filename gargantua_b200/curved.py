@@ -120,6 +120,8 @@ class RenderOptions:
     integrator: Optional[RK45Integrator] = None
     precision: int = abi.GG_PREC_FP64
     attempt_budget: int = 0
+    row_offset: int = 0   # with row_step > 1: trace rows row_offset, row_offset + row_step, ...
+    row_step: int = 1
 
     def to_c(self) -> abi.gg_render_opts_t:
         o = abi.gg_render_opts_t()
@@ -133,6 +135,8 @@ class RenderOptions:
         else:
             o.sky, o.sky_rows, o.sky_cols, o.sky_seed = abi.GG_SKY_PROCEDURAL, 18, 36, 0
         o.attempt_budget = int(self.attempt_budget)
+        o.row_offset = int(self.row_offset)
+        o.row_step = max(1, int(self.row_step))
         return o
 
 
@@ -154,7 +158,15 @@ class Scene:
 
     @property
     def n_samples(self) -> int:
-        return self.width * self.height * self.spp
+        return self.width * self.rows * self.spp
+
+    @property
+    def rows(self) -> int:
+        """Image rows this render traces (all of them unless the options
+        select every row_step-th row from row_offset)."""
+        step = max(1, int(self.options.row_step))
+        off = int(self.options.row_offset)
+        return 0 if off >= self.height else (self.height - off + step - 1) // step
 
     def integrator_c(self) -> abi.gg_integrator_t:
         integ = self.options.integrator or renderer_integrator()
@@ -228,7 +240,7 @@ class Renderer:
 
     def render(self, scene: Scene, rays: bool = False):
         """Synchronous render into host memory: (image, RayOutputs or None)."""
-        img = np.zeros((scene.height, scene.width, 3), np.uint8)
+        img = np.zeros((scene.rows, scene.width, 3), np.uint8)
         out = RayOutputs(scene.n_samples) if rays else None
         st = self._lib.gg_render(self._h, *scene.c_args(), img.ctypes.data_as(C.c_void_p),
                                  C.byref(out.struct()) if out else None)
@@ -237,7 +249,7 @@ class Renderer:
 
     def render_into(self, scene: Scene, rgb_host: np.ndarray) -> None:
         """Synchronous render into a caller-owned (e.g. pinned) uint8 host buffer."""
-        assert rgb_host.dtype == np.uint8 and rgb_host.size >= scene.width * scene.height * 3
+        assert rgb_host.dtype == np.uint8 and rgb_host.size >= scene.width * scene.rows * 3
         st = self._lib.gg_render(self._h, *scene.c_args(), rgb_host.ctypes.data_as(C.c_void_p),
                                  None)
         abi.check(st, "gg_render")

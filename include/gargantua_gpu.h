@@ -125,9 +125,15 @@ typedef struct gg_render_opts_t {
   int32_t sky;               /* GG_SKY_*                                    */
   uint32_t sky_rows;         /* checkerboard cells in theta (18)            */
   uint32_t sky_cols;         /* checkerboard cells in phi (36)              */
-  uint32_t reserved;
+  uint32_t row_offset;       /* with row_step: first image row traced       */
   uint64_t sky_seed;
   uint64_t attempt_budget;   /* 0: unlimited; else GG_ERR_BUDGET past it    */
+  /* row_step > 1: trace only image rows row_offset, row_offset + row_step,
+   * ... (one GPU's share of a frame split across GPUs, interleaved so every
+   * share gets rows through the shadow); the image and per-sample outputs
+   * then hold those rows only, in order.  0 or 1: every row. */
+  uint32_t row_step;
+  uint32_t reserved;
 } gg_render_opts_t;
 
 /* ---- per-sample outcome (RayOutcome + final GeodesicState) ------------- */

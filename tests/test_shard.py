@@ -1,0 +1,83 @@
+"""A frame split across GPUs by interleaved rows (gargantua_b200.shard).
+
+CPU: the row partition and the assembly, and the gather itself with two
+gloo ranks (127.0.0.1).  GPU: the shards a rank would render, stitched,
+equal the unsplit render byte for byte (each ray's arithmetic does not
+depend on which rows share its launch; jitter is keyed by the sample's
+index in the whole image).
+"""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import pytest
+
+from gargantua_b200 import abi, shard, workloads
+
+
+@pytest.mark.parametrize("height,world", [(8, 2), (7, 2), (5, 3), (2, 4)])
+def test_partition_and_assembly(height, world):
+    full = np.arange(height * 3 * 3, dtype=np.int64).reshape(height, 3, 3)
+    parts = [full[k::world] for k in range(world)]
+    assert sum(shard.rows_of(height, k, world) for k in range(world)) == height
+    assert [p.shape[0] for p in parts] == [shard.rows_of(height, k, world) for k in range(world)]
+    assert np.array_equal(shard.assemble(parts, height), full)
+
+
+def _gather_worker(rank, world, port, height, q):
+    import torch
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        full = np.arange(height * 4 * 3, dtype=np.uint8).reshape(height, 4, 3)
+        local = torch.from_numpy(np.ascontiguousarray(full[rank::world]))
+        got = shard.gather_rows(local, height, rank, world)
+        if rank == 0:
+            q.put(bool(np.array_equal(got, full)))
+        else:
+            q.put(got is None)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("height", [9, 8])
+def test_gather_two_gloo_ranks(height):
+    import socket
+
+    import torch.multiprocessing as mp
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_gather_worker, args=(r, 2, port, height, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+    assert all(p.exitcode == 0 for p in procs)
+    assert all(q.get(timeout=10) for _ in procs)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("form", ["fp64", "mixed", "jitter"])
+def test_shards_equal_the_unsplit_render(renderer, form):
+    if form == "mixed":
+        scene = workloads.kerr_thin_1080p(precision=abi.GG_PREC_MIXED,
+                                          stepper=abi.GG_STEPPER_DP45)
+        scene.width, scene.height = 192, 108
+    elif form == "jitter":
+        scene = workloads.kerr_stress_4k(side=48, spp=4)
+    else:
+        scene = workloads.schwarzschild_thin_256()
+    full, _ = renderer.render(scene)
+    world = 3
+    parts = []
+    for k in range(world):
+        img, _ = renderer.render(shard.shard_scene(scene, k, world))
+        assert img.shape[0] == shard.rows_of(scene.height, k, world)
+        parts.append(img)
+    assert np.array_equal(shard.assemble(parts, scene.height), full)
