@@ -38,6 +38,7 @@ GG_STEPPER_DP45 = 1
 GG_BATCH_VARIANTS = 6
 GG_SKY_PROCEDURAL = 0
 GG_SKY_CHECKER = 1
+GG_SKY_HDRI = 2
 
 GG_CLASS_HORIZON = 0
 GG_CLASS_ESCAPED = 1
@@ -145,6 +146,7 @@ _SIGNATURES = {
     "gg_batch_autotune": (C.c_int, [C.c_void_p, P(gg_scene_t), C.c_uint32, P(gg_integrator_t),
                                     P(gg_render_opts_t), P(C.c_int), P(C.c_double)]),
     "gg_batch_set_variant": (C.c_int, [C.c_void_p, C.c_int]),
+    "gg_set_hdri": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_float]),
     "gg_forward_ckpt": (C.c_int, [C.c_void_p, P(gg_metric_t), C.c_double, C.c_double, C.c_double,
                                   C.c_double, P(gg_disk_t), P(gg_integrator_t),
                                   P(gg_render_opts_t), C.c_uint32, C.c_uint32, C.c_void_p,

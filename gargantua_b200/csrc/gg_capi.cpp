@@ -63,6 +63,11 @@ struct gg_ctx {
   size_t diff_ckpt_cap = 0;
   double* diff_grad = nullptr;       // 5 doubles, device
   double* diff_grad_host = nullptr;  // pinned
+  // equirectangular sky map (gg_set_hdri), RGB float texels on the device
+  float* hdri = nullptr;
+  size_t hdri_cap = 0;
+  uint32_t hdri_w = 0, hdri_h = 0;
+  float hdri_intensity = 1.f;
   bool pending = false;            // stats of the last device-pointer render not read yet
   gg_stats_t last{};
   std::mutex mu;
@@ -195,7 +200,8 @@ int validate(const gg_metric_t* metric, const gg_camera_t* camera, const gg_disk
     return GG_ERR_INVALID_ARG;
   if (integ->stepper != GG_STEPPER_REFERENCE && integ->stepper != GG_STEPPER_DP45)
     return GG_ERR_INVALID_ARG;
-  if (opts->sky != GG_SKY_PROCEDURAL && opts->sky != GG_SKY_CHECKER) return GG_ERR_INVALID_ARG;
+  if (opts->sky != GG_SKY_PROCEDURAL && opts->sky != GG_SKY_CHECKER && opts->sky != GG_SKY_HDRI)
+    return GG_ERR_INVALID_ARG;
   if (opts->sky == GG_SKY_CHECKER && (opts->sky_rows < 1 || opts->sky_cols < 1))
     return GG_ERR_INVALID_ARG;
   if (width < 1 || height < 1) return GG_ERR_INVALID_ARG;
@@ -329,6 +335,18 @@ void build_params(const gg_metric_t* metric, const gg_camera_t* camera, const gg
   P.cell_w = (2.0 * kPi) / (double)(opts->sky_cols ? opts->sky_cols : 1);
   P.attempt_budget = opts->attempt_budget;
   *out = P;
+}
+
+// The context's sky map into P for GG_SKY_HDRI renders; no map set is an
+// invalid argument.
+int attach_sky_map(const gg_ctx* c, DevParams* P) {
+  if (P->sky != gg::kSkyHdri) return GG_OK;
+  if (!c->hdri) return GG_ERR_INVALID_ARG;
+  P->hdri = c->hdri;
+  P->hdri_w = c->hdri_w;
+  P->hdri_h = c->hdri_h;
+  P->hdri_intensity = c->hdri_intensity;
+  return GG_OK;
 }
 
 int grow_pinned(void** buf, size_t* cap, size_t need) {
@@ -469,7 +487,7 @@ int batch_prepare(gg_ctx* c, const gg_scene_t* scenes, uint32_t n, const gg_inte
   if (integ->precision != GG_PREC_MIXED || integ->stepper != GG_STEPPER_DP45)
     return GG_ERR_UNSUPPORTED;
   if (opts->samples_per_axis > 1 || opts->jitter_spp > 0 || opts->attempt_budget != 0 ||
-      opts->row_step > 1)
+      opts->row_step > 1 || opts->sky == GG_SKY_HDRI)
     return GG_ERR_UNSUPPORTED;
   const int kind = scenes[0].metric.kind, disk_kind = scenes[0].disk.kind;
   if (disk_kind != GG_DISK_NONE && disk_kind != GG_DISK_THIN) return GG_ERR_UNSUPPORTED;
@@ -801,6 +819,7 @@ GG_API int gg_destroy(gg_ctx* c) {
   if (c->diff_ckpt) cudaFree(c->diff_ckpt);
   if (c->diff_grad) cudaFree(c->diff_grad);
   if (c->diff_grad_host) cudaFreeHost(c->diff_grad_host);
+  if (c->hdri) cudaFree(c->hdri);
   if (c->ctl) cudaFree(c->ctl);
   if (c->ctl_host) cudaFreeHost(c->ctl_host);
   if (c->ev_start) cudaEventDestroy(c->ev_start);
@@ -840,6 +859,8 @@ GG_API int gg_render_device(gg_ctx* c, const gg_metric_t* metric, const gg_camer
   DevParams P;
   build_params(metric, camera, disk, integ, opts, width, height, &P);
   Lock lock(c);
+  const int sky = attach_sky_map(c, &P);
+  if (sky != GG_OK) return sky;
   DevOutputs O;
   std::memset(&O, 0, sizeof(O));
   if (rays_dev) {
@@ -933,6 +954,28 @@ GG_API int gg_batch_autotune(gg_ctx* c, const gg_scene_t* scenes, uint32_t n,
   return GG_OK;
 }
 
+GG_API int gg_set_hdri(gg_ctx* c, const float* rgb, uint32_t width, uint32_t height,
+                       float intensity) {
+  if (!c || !rgb || width < 1 || height < 1 || !std::isfinite(intensity))
+    return GG_ERR_INVALID_ARG;
+  const uint64_t texels = (uint64_t)width * height;
+  if (texels > (1ull << 32)) return GG_ERR_INVALID_ARG;
+  const size_t bytes = texels * 3 * sizeof(float);
+  Lock lock(c);
+  // renders in flight may read the old map
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return GG_ERR_CUDA;
+  if (cudaEventSynchronize(c->ev_done) != cudaSuccess) return GG_ERR_CUDA;
+  void* buf = c->hdri;
+  int st = grow(&buf, &c->hdri_cap, bytes);
+  c->hdri = static_cast<float*>(buf);
+  if (st != GG_OK) return st;
+  if (cudaMemcpy(c->hdri, rgb, bytes, cudaMemcpyHostToDevice) != cudaSuccess) return GG_ERR_CUDA;
+  c->hdri_w = width;
+  c->hdri_h = height;
+  c->hdri_intensity = intensity;
+  return GG_OK;
+}
+
 GG_API int gg_batch_set_variant(gg_ctx* c, int variant) {
   if (!c || variant < 0 || variant >= GG_BATCH_VARIANTS) return GG_ERR_INVALID_ARG;
   Lock lock(c);
@@ -954,7 +997,7 @@ GG_API int gg_forward_ckpt(gg_ctx* c, const gg_metric_t* metric, double r_cam,
   if (metric->kind != GG_METRIC_KERR || disk->kind != GG_DISK_THIN ||
       integ->precision != GG_PREC_FP64 || integ->stepper != GG_STEPPER_DP45 ||
       opts->samples_per_axis > 1 || opts->jitter_spp > 0 || opts->attempt_budget != 0 ||
-      opts->row_step > 1)
+      opts->row_step > 1 || opts->sky == GG_SKY_HDRI)
     return GG_ERR_UNSUPPORTED;
   Lock lock(c);
   DevParams P;
@@ -1022,6 +1065,8 @@ GG_API int gg_render(gg_ctx* c, const gg_metric_t* metric, const gg_camera_t* ca
   DevParams P;
   build_params(metric, camera, disk, integ, opts, width, height, &P);
   Lock lock(c);
+  const int sky = attach_sky_map(c, &P);
+  if (sky != GG_OK) return sky;
   const uint64_t n = P.n_rays;
   const size_t n_pix = (size_t)width * P.rows;
 

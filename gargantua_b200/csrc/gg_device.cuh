@@ -889,16 +889,58 @@ GG_DEV void init_ray(const DevParams& P, double u, double v, Ray& R) {
 // ---------------------------------------------------------------------------
 // Shading (crates/raytracer/src/curved/renderer.rs:44-80, sky.rs:26-40).
 // ---------------------------------------------------------------------------
-GG_DEV void procedural_sky(const double v[4], double rgb[3]) {
-  // spatial_dir (tracer.rs:185-189)
+// spatial_dir (tracer.rs:185-189): (v^r, v^theta, v^phi) normalised as a
+// Cartesian 3-vector, (1, 0, 0) for a zero vector.
+GG_DEV void spatial_dir(const double v[4], double& d0, double& d1, double& d2) {
   const double sx = v[1], sy = v[2], sz = v[3];
   const double n = __dsqrt_rn(add_rn(add_rn(mul_rn(sx, sx), mul_rn(sy, sy)), mul_rn(sz, sz)));
-  double d0 = 1.0, d1 = 0.0, d2 = 0.0;
+  d0 = 1.0;
+  d1 = 0.0;
+  d2 = 0.0;
   if (n > 0.0) {
     d0 = __ddiv_rn(sx, n);
     d1 = __ddiv_rn(sy, n);
     d2 = __ddiv_rn(sz, n);
   }
+}
+
+// HdriSky::sample and fetch (sky.rs:88-123): theta = acos(z), phi =
+// atan2(y, x), u = phi / (2 pi) + 1/2, v = theta / pi; bilinear in f32 with
+// wrap in x and clamp in y, in the reference's order without contraction.
+GG_DEV void hdri_sky(const DevParams& P, const double v[4], double rgb[3]) {
+  double d0, d1, d2;
+  spatial_dir(v, d0, d1, d2);
+  const double z = fmin(fmax(d2, -1.0), 1.0);
+  const double theta = acos(z);
+  const double phi = atan2(d1, d0);
+  constexpr double kFrac1Pi = 0.318309886183790671538;
+  const double u = add_rn(mul_rn(mul_rn(phi, kFrac1Pi), 0.5), 0.5);
+  const double vv = mul_rn(theta, kFrac1Pi);
+  const double w = (double)P.hdri_w, h = (double)P.hdri_h;
+  double fx = fmod(mul_rn(u, w), w);
+  if (fx < 0.0) fx = add_rn(fx, w);
+  const double fy = fmin(fmax(mul_rn(vv, h), 0.0), sub_rn(h, 1.0));
+  const uint32_t x0 = (uint32_t)floor(fx) % P.hdri_w;
+  const uint32_t y0 = (uint32_t)floor(fy);
+  const uint32_t x1 = (x0 + 1) % P.hdri_w;
+  const uint32_t y1 = y0 + 1 < P.hdri_h ? y0 + 1 : P.hdri_h - 1;
+  const float tx = (float)sub_rn(fx, floor(fx));
+  const float ty = (float)sub_rn(fy, floor(fy));
+  const float* p00 = P.hdri + 3 * ((uint64_t)y0 * P.hdri_w + x0);
+  const float* p10 = P.hdri + 3 * ((uint64_t)y0 * P.hdri_w + x1);
+  const float* p01 = P.hdri + 3 * ((uint64_t)y1 * P.hdri_w + x0);
+  const float* p11 = P.hdri + 3 * ((uint64_t)y1 * P.hdri_w + x1);
+  auto lerp = [](float a, float b, float t) { return __fadd_rn(a, __fmul_rn(__fsub_rn(b, a), t)); };
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const float px = lerp(lerp(p00[c], p10[c], tx), lerp(p01[c], p11[c], tx), ty);
+    rgb[c] = (double)__fmul_rn(px, P.hdri_intensity);
+  }
+}
+
+GG_DEV void procedural_sky(const double v[4], double rgb[3]) {
+  double d0, d1, d2;
+  spatial_dir(v, d0, d1, d2);
   auto hash = [](double x) -> uint64_t {
     return (uint64_t)__double_as_longlong(x) * 6364136223846793005ULL +
            1442695040888963407ULL;

@@ -68,7 +68,9 @@ extern "C" GG_API int gg_render_device_noalloc(const gg_metric_t* metric,
                                                const gg_ray_out_t* rays_dev, void* stream) {
   const int v = gg::validate_render(metric, camera, disk, integ, opts, width, height);
   if (v != GG_OK) return v;
-  if (integ->precision != GG_PREC_FP64 || opts->attempt_budget != 0) return GG_ERR_UNSUPPORTED;
+  if (integ->precision != GG_PREC_FP64 || opts->attempt_budget != 0 ||
+      opts->sky == GG_SKY_HDRI)  // the map belongs to a context
+    return GG_ERR_UNSUPPORTED;
   gg::DevParams P;
   gg::make_params(metric, camera, disk, integ, opts, width, height, &P);
   const bool want_image = rgb_dev != nullptr;

@@ -14,7 +14,7 @@ namespace gg {
 
 enum : int { kMetricSchwarzschild = 0, kMetricKerr = 1 };
 enum : int { kDiskNone = 0, kDiskVolumetric = 1, kDiskThin = 2 };
-enum : int { kSkyProcedural = 0, kSkyChecker = 1 };
+enum : int { kSkyProcedural = 0, kSkyChecker = 1, kSkyHdri = 2 };
 enum : int { kClsHorizon = 0, kClsEscaped = 1, kClsDisk = 2, kClsMaxSteps = 3, kClsBudget = 4 };
 enum : int { kStepperReference = 0, kStepperDP45 = 1 };
 
@@ -64,6 +64,10 @@ struct DevParams {
   uint32_t pad2;
   uint64_t sky_seed;
   double cell_h, cell_w;
+  const float* hdri;  // GG_SKY_HDRI: the context's map, hdri_w x hdri_h RGB texels
+  uint32_t hdri_w, hdri_h;
+  float hdri_intensity;
+  float pad_hdri;
   // control
   uint64_t attempt_budget;
   double inv_spp;

@@ -54,6 +54,8 @@ __device__ __noinline__ void finish_sample(const DevParams& P, const DevOutputs&
     } else if (cls == kClsEscaped) {
       if (P.sky == kSkyChecker)
         checker_sky(P, sky_th, sky_ph, lin);
+      else if (P.sky == kSkyHdri)
+        hdri_sky(P, R.v, lin);
       else
         procedural_sky(R.v, lin);
     } else if (cls == kClsDisk) {

@@ -5,6 +5,9 @@
 ``uint8`` array of shape (height, width, 3), the ``RgbImage`` layout.  They
 run the CUDA library; there is no CPU path.
 
+``HdriSky`` is the reference's equirectangular environment map
+(crates/raytracer/src/curved/sky.rs:43-123), sampled on the GPU.
+
 Extensions beyond the reference (all opt-in through ``RenderOptions`` or
 ``Scene``): a thin equatorial disk, a seeded checkerboard sky, seeded
 jittered samples, a configurable step budget and integrator, the mixed
@@ -107,13 +110,62 @@ class CheckerSky:
     seed: int = 0
 
 
+class HdriSky:
+    """Equirectangular environment map (sky.rs:43-123): linear RGB float32
+    texels, shape (height, width, 3), row 0 at the +z pole, columns wrapping
+    in azimuth; bilinear with wrap in x and clamp in y, times ``intensity``.
+
+    A Renderer uploads the map the first time a render meets this object
+    (and again after ``with_intensity`` or ``set_pixels``)."""
+
+    def __init__(self, pixels, intensity: float = 1.0):
+        self.set_pixels(pixels)
+        self.intensity = float(intensity)
+
+    @classmethod
+    def from_pixels(cls, width: int, height: int, pixels) -> "HdriSky":
+        """HdriSky::from_pixels (sky.rs:75-78): width*height RGB triples, row-major."""
+        px = np.asarray(pixels, np.float32)
+        if px.size != width * height * 3:
+            raise ValueError("pixel buffer size mismatch")
+        return cls(px.reshape(height, width, 3))
+
+    @classmethod
+    def from_file(cls, path) -> "HdriSky":
+        """HdriSky::from_file (sky.rs:59-71) for Radiance .hdr files."""
+        from .hdr import read_hdr
+        return cls(read_hdr(path))
+
+    def with_intensity(self, intensity: float) -> "HdriSky":
+        self.intensity = float(intensity)
+        return self
+
+    def set_pixels(self, pixels) -> None:
+        px = np.ascontiguousarray(pixels, np.float32)
+        if px.ndim != 3 or px.shape[2] != 3 or px.shape[0] < 1 or px.shape[1] < 1:
+            raise ValueError("HdriSky pixels must be (height, width, 3)")
+        self.pixels = px
+        self.version = getattr(self, "version", 0) + 1
+
+    @property
+    def width(self) -> int:
+        return self.pixels.shape[1]
+
+    @property
+    def height(self) -> int:
+        return self.pixels.shape[0]
+
+    def key(self):
+        return (id(self), self.version, self.intensity)
+
+
 @dataclass
 class RenderOptions:
     """``RenderOptions`` (renderer.rs:17-26) plus the extensions listed above."""
 
     samples_per_axis: int = 1
     show_progress: bool = False
-    sky: Union[ProceduralSky, CheckerSky, None] = None
+    sky: Union[ProceduralSky, CheckerSky, HdriSky, None] = None
     jitter_spp: int = 0
     seed: int = 0
     max_steps: int = 5000
@@ -132,6 +184,8 @@ class RenderOptions:
         if isinstance(sky, CheckerSky):
             o.sky, o.sky_rows, o.sky_cols = abi.GG_SKY_CHECKER, sky.rows, sky.cols
             o.sky_seed = int(sky.seed) & (2**64 - 1)
+        elif isinstance(sky, HdriSky):
+            o.sky, o.sky_rows, o.sky_cols, o.sky_seed = abi.GG_SKY_HDRI, 18, 36, 0
         else:
             o.sky, o.sky_rows, o.sky_cols, o.sky_seed = abi.GG_SKY_PROCEDURAL, 18, 36, 0
         o.attempt_budget = int(self.attempt_budget)
@@ -218,6 +272,7 @@ class Renderer:
         h = C.c_void_p()
         abi.check(self._lib.gg_create(C.byref(h), int(device)), "gg_create")
         self._h = h
+        self._hdri_key = None
 
     def close(self) -> None:
         if self._h:
@@ -238,10 +293,23 @@ class Renderer:
     def stream(self) -> int:
         return self._lib.gg_stream(self._h) or 0
 
+    def set_hdri(self, sky: HdriSky) -> None:
+        """Uploads `sky`'s map to this context (gg_set_hdri)."""
+        px = sky.pixels
+        abi.check(self._lib.gg_set_hdri(self._h, px.ctypes.data_as(C.c_void_p), px.shape[1],
+                                        px.shape[0], C.c_float(sky.intensity)), "gg_set_hdri")
+        self._hdri_key = sky.key()
+
+    def _sky_map(self, scene: Scene) -> None:
+        sky = scene.options.sky
+        if isinstance(sky, HdriSky) and sky.key() != self._hdri_key:
+            self.set_hdri(sky)
+
     def render(self, scene: Scene, rays: bool = False):
         """Synchronous render into host memory: (image, RayOutputs or None)."""
         img = np.zeros((scene.rows, scene.width, 3), np.uint8)
         out = RayOutputs(scene.n_samples) if rays else None
+        self._sky_map(scene)
         st = self._lib.gg_render(self._h, *scene.c_args(), img.ctypes.data_as(C.c_void_p),
                                  C.byref(out.struct()) if out else None)
         abi.check(st, "gg_render")
@@ -250,6 +318,7 @@ class Renderer:
     def render_into(self, scene: Scene, rgb_host: np.ndarray) -> None:
         """Synchronous render into a caller-owned (e.g. pinned) uint8 host buffer."""
         assert rgb_host.dtype == np.uint8 and rgb_host.size >= scene.width * scene.rows * 3
+        self._sky_map(scene)
         st = self._lib.gg_render(self._h, *scene.c_args(), rgb_host.ctypes.data_as(C.c_void_p),
                                  None)
         abi.check(st, "gg_render")
@@ -266,6 +335,7 @@ class Renderer:
         """Enqueue a render writing device pointers (no synchronisation).
 
         ``stream`` is a cudaStream_t handle; None or 0 is CUDA's default stream."""
+        self._sky_map(scene)
         st = self._lib.gg_render_device(self._h, *scene.c_args(), C.c_void_p(rgb_dev),
                                         C.byref(rays_dev) if rays_dev is not None else None,
                                         C.c_void_p(stream or 0))
@@ -352,5 +422,5 @@ def render_with_disk(metric: Metric, camera: Camera, disk: Union[AccretionDisk, 
     return _renderer().render(scene)[0]
 
 
-__all__ = ["Camera", "AccretionDisk", "ThinDisk", "ProceduralSky", "CheckerSky",
+__all__ = ["Camera", "AccretionDisk", "ThinDisk", "ProceduralSky", "CheckerSky", "HdriSky",
            "RenderOptions", "Scene", "RayOutputs", "Renderer", "render", "render_with_disk"]

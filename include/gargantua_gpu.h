@@ -117,6 +117,7 @@ typedef struct gg_integrator_t {
 /* ---- render options (raytracer::curved::RenderOptions) ----------------- */
 #define GG_SKY_PROCEDURAL 0 /* hashed starfield over a blue gradient          */
 #define GG_SKY_CHECKER 1    /* seeded checkerboard over (theta, phi) cells     */
+#define GG_SKY_HDRI 2       /* equirectangular map of the context (gg_set_hdri) */
 
 typedef struct gg_render_opts_t {
   uint32_t samples_per_axis; /* stratified supersampling, spa*spa per pixel */
@@ -326,6 +327,16 @@ GG_API int gg_forward_ckpt(gg_ctx* ctx, const gg_metric_t* metric, double r_cam,
  * the emissivity); sky and horizon pixels are piecewise constant in p.
  * Recomputes trajectories from the checkpoints.  Synchronises `stream`. */
 GG_API int gg_backward(gg_ctx* ctx, const double* dl_drgb_dev, double grad[5], void* stream);
+
+/* ---- sky map ----------------------------------------------------------- */
+/* Sets the context's equirectangular sky map, raytracer::curved::HdriSky
+ * (crates/raytracer/src/curved/sky.rs:43-123): width*height linear RGB float
+ * texels, row-major, row 0 = the +z pole, columns wrapping in azimuth
+ * (decoding the .hdr file stays with the caller).  Copied to the device;
+ * renders with opts.sky = GG_SKY_HDRI sample it bilinearly (wrap in x, clamp
+ * in y) at the escape direction, scaled by `intensity`. */
+GG_API int gg_set_hdri(gg_ctx* ctx, const float* rgb, uint32_t width, uint32_t height,
+                       float intensity);
 
 /* ---- measurement ------------------------------------------------------- */
 /* FMA throughput of the context's device in FLOP/s (an FMA counts 2), best

@@ -989,6 +989,57 @@ inline void checker_sky(double theta, double phi, uint32_t rows, uint32_t cols, 
   }
 }
 
+// HdriSky (sky.rs:43-123): equirectangular linear RGB f32 texels, row 0 at
+// the +z pole, bilinear with wrap in x and clamp in y, scaled by intensity.
+struct HdriMap {
+  const float* px = nullptr;  // width * height * 3, row-major
+  uint32_t width = 0, height = 0;
+  float intensity = 1.f;
+};
+
+// HdriSky::fetch (sky.rs:85-105)
+inline void hdri_fetch(const HdriMap& m, double u, double v, float out[3]) {
+  const double w = (double)m.width, h = (double)m.height;
+  double fx = std::fmod(u * w, w);  // rem_euclid
+  if (fx < 0.0) fx += w;
+  double fy = v * h;
+  if (fy < 0.0) fy = 0.0;
+  if (fy > h - 1.0) fy = h - 1.0;
+  const size_t x0 = (size_t)std::floor(fx) % m.width;
+  const size_t y0 = (size_t)std::floor(fy);
+  const size_t x1 = (x0 + 1) % m.width;
+  const size_t y1 = y0 + 1 < m.height ? y0 + 1 : m.height - 1;
+  const float tx = (float)(fx - std::floor(fx));
+  const float ty = (float)(fy - std::floor(fy));
+  auto at = [&](size_t y, size_t x, int c) { return m.px[3 * (y * m.width + x) + c]; };
+  auto lerp = [](float a, float b, float t) {
+    volatile float d = b - a;  // no contraction into an fma
+    volatile float p = d * t;
+    return a + p;
+  };
+  for (int c = 0; c < 3; ++c)
+    out[c] = lerp(lerp(at(y0, x0, c), at(y0, x1, c), tx), lerp(at(y1, x0, c), at(y1, x1, c), tx),
+                  ty);
+}
+
+// HdriSky::sample (sky.rs:108-122)
+inline void hdri_sky(const HdriMap& m, const V3& dir, double rgb[3]) {
+  double z = dir[2];
+  if (z < -1.0) z = -1.0;
+  if (z > 1.0) z = 1.0;
+  const double theta = std::acos(z);
+  const double phi = std::atan2(dir[1], dir[0]);
+  constexpr double kFrac1Pi = 0.318309886183790671538;
+  const double u = phi * kFrac1Pi * 0.5 + 0.5;
+  const double v = theta * kFrac1Pi;
+  float px[3];
+  hdri_fetch(m, u, v, px);
+  for (int c = 0; c < 3; ++c) {
+    volatile float s = px[c] * m.intensity;
+    rgb[c] = (double)s;
+  }
+}
+
 inline void disk_color(double intensity, double rgb[3]) {  // renderer.rs:62-66
   double x = intensity / (1.0 + intensity);
   rgb[0] = std::pow(x, 0.5);
@@ -1011,7 +1062,7 @@ inline uint8_t encode_channel(double c) {  // renderer.rs:69-80
 // ---------------------------------------------------------------------------
 enum RayClass { kClsHorizon = 0, kClsEscaped = 1, kClsDisk = 2, kClsMaxSteps = 3 };
 enum DiskKind { kDiskNone = 0, kDiskVolumetric = 1, kDiskThin = 2 };
-enum SkyKind { kSkyProcedural = 0, kSkyChecker = 1 };
+enum SkyKind { kSkyProcedural = 0, kSkyChecker = 1, kSkyHdri = 2 };
 
 struct ThinDisk {  // EXTENSION
   double r_inner = 6.0, r_outer = 20.0, emissivity_index = 3.0;
@@ -1026,6 +1077,7 @@ struct TraceSetup {
   int sky = kSkyProcedural;
   uint32_t sky_rows = 18, sky_cols = 36;
   uint64_t sky_seed = 0;
+  HdriMap hdri;
 };
 
 struct Sample {
@@ -1067,6 +1119,8 @@ void shade(const M&, const TraceSetup& S, Sample& o) {  // renderer.rs:44-53
         const double th = at_cross ? o.cross[2] : o.st.position[2];
         const double ph = at_cross ? o.cross[3] : o.st.position[3];
         checker_sky(th, ph, S.sky_rows, S.sky_cols, S.sky_seed, o.rgb);
+      } else if (S.sky == kSkyHdri) {
+        hdri_sky(S.hdri, spatial_dir(o.st.velocity), o.rgb);
       } else {
         procedural_sky(spatial_dir(o.st.velocity), o.rgb);
       }

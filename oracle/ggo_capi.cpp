@@ -45,6 +45,10 @@ RK45 make_rk45(const gg_integrator_t* in) {
   return k;
 }
 
+// The sky map GG_SKY_HDRI renders sample (ggo_set_hdri); one per process.
+std::vector<float> g_hdri_px;
+HdriMap g_hdri;
+
 TraceSetup make_setup(const gg_disk_t* disk, const gg_integrator_t* integ,
                       const gg_render_opts_t* opts) {
   TraceSetup S;
@@ -65,6 +69,7 @@ TraceSetup make_setup(const gg_disk_t* disk, const gg_integrator_t* integ,
   S.sky_rows = opts->sky_rows;
   S.sky_cols = opts->sky_cols;
   S.sky_seed = opts->sky_seed;
+  S.hdri = g_hdri;
   return S;
 }
 
@@ -408,6 +413,22 @@ GGO_API void ggo_procedural_sky(const double dir[3], double rgb[3]) {
 GGO_API void ggo_checker_sky(double theta, double phi, uint32_t rows, uint32_t cols,
                              uint64_t seed, double rgb[3]) {
   checker_sky(theta, phi, rows, cols, seed, rgb);
+}
+
+// Sets the map of GG_SKY_HDRI renders (copied); returns 0, or -1 for no texels.
+GGO_API int ggo_set_hdri(const float* rgb, uint32_t width, uint32_t height, float intensity) {
+  if (!rgb || width < 1 || height < 1) return -1;
+  g_hdri_px.assign(rgb, rgb + (size_t)width * height * 3);
+  g_hdri.px = g_hdri_px.data();
+  g_hdri.width = width;
+  g_hdri.height = height;
+  g_hdri.intensity = intensity;
+  return 0;
+}
+
+// HdriSky::sample of the map set by ggo_set_hdri at direction dir.
+GGO_API void ggo_hdri_sky(const double dir[3], double rgb[3]) {
+  hdri_sky(g_hdri, V3{{dir[0], dir[1], dir[2]}}, rgb);
 }
 
 GGO_API void ggo_disk_color(double intensity, double rgb[3]) { disk_color(intensity, rgb); }

@@ -80,6 +80,8 @@ def lib(variant: str = "plain") -> C.CDLL:
             "ggo_checker_sky": (None, [C.c_double, C.c_double, C.c_uint32, C.c_uint32,
                                        C.c_uint64, C.c_void_p]),
             "ggo_disk_color": (None, [C.c_double, C.c_void_p]),
+            "ggo_set_hdri": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_float]),
+            "ggo_hdri_sky": (None, [C.c_void_p, C.c_void_p]),
             "ggo_encode_srgb": (None, [C.c_void_p, C.c_void_p]),
             "ggo_splitmix64": (C.c_uint64, [C.c_uint64]),
             "ggo_sample_uv": (None, [P(abi.gg_render_opts_t), C.c_uint32, C.c_uint32,
@@ -102,6 +104,28 @@ def _ptr(a: np.ndarray):
 from gargantua_b200.curved import RayOutputs as RayArrays  # noqa: E402
 
 
+def set_hdri(sky, variant: str = "plain") -> None:
+    """Makes `sky` (a gargantua_b200.curved.HdriSky) the map of GG_SKY_HDRI renders."""
+    px = np.ascontiguousarray(sky.pixels, np.float32)
+    if lib(variant).ggo_set_hdri(_ptr(px), px.shape[1], px.shape[0], C.c_float(sky.intensity)):
+        raise ValueError("empty sky map")
+
+
+def hdri_sample(sky, direction) -> np.ndarray:
+    """HdriSky::sample (sky.rs:108-122) of `sky` at a direction (3 floats)."""
+    set_hdri(sky)
+    d = np.ascontiguousarray(direction, np.float64)
+    out = np.zeros(3)
+    lib().ggo_hdri_sky(_ptr(d), _ptr(out))
+    return out
+
+
+def _sky_map(scene, variant: str) -> None:
+    from gargantua_b200.curved import HdriSky
+    if isinstance(scene.options.sky, HdriSky):
+        set_hdri(scene.options.sky, variant)
+
+
 def render(scene, threads: int = 0, rays: bool = True, variant: str = "plain"):
     """Render ``scene`` (a ``gargantua_b200.curved.Scene``) on the CPU oracle.
 
@@ -110,6 +134,7 @@ def render(scene, threads: int = 0, rays: bool = True, variant: str = "plain"):
     n = w * h * scene.spp
     img = np.zeros((h, w, 3), np.uint8)
     ra = RayArrays(n) if rays else None
+    _sky_map(scene, variant)
     st = lib(variant).ggo_render(*scene.c_args(), _ptr(img), C.byref(ra.struct()) if ra else None,
                           threads)
     abi.check(st, "ggo_render")
@@ -120,6 +145,7 @@ def trace_samples(scene, index: np.ndarray, threads: int = 0,
                   variant: str = "plain") -> RayArrays:
     index = np.ascontiguousarray(index, np.uint64)
     ra = RayArrays(len(index))
+    _sky_map(scene, variant)
     st = lib(variant).ggo_trace_samples(*scene.c_args(), _ptr(index), len(index),
                                  C.byref(ra.struct()), threads)
     abi.check(st, "ggo_trace_samples")
@@ -128,6 +154,7 @@ def trace_samples(scene, index: np.ndarray, threads: int = 0,
 
 def trace_uv(scene, u: float, v: float) -> RayArrays:
     ra = RayArrays(1)
+    _sky_map(scene, "plain")
     st = lib().ggo_trace_uv(*scene.c_args()[:5], u, v, C.byref(ra.struct()))
     abi.check(st, "ggo_trace_uv")
     return ra
