@@ -223,7 +223,10 @@ def time_e2e(r, scene, steps, warmup, world):
     return el
 
 
-def cpu_baseline(scene, target_s: float = 10.0) -> dict:
+def cpu_baseline(scene, target_s: float = 10.0, what: str = "the 1920x1080 frame") -> dict:
+    """The oracle (C++ restatement of the reference renderer, rows over all
+    host threads) on a seeded subset of `scene`'s samples sized for about
+    `target_s` seconds; geodesics/s extrapolated from the subset."""
     import numpy as np
     from oracle import oracle
     rng = np.random.default_rng(0)
@@ -238,8 +241,36 @@ def cpu_baseline(scene, target_s: float = 10.0) -> dict:
     oracle.trace_samples(scene, idx, threads=threads)
     el = time.perf_counter() - t0
     return {"value": n / el, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{n} seeded rays of the 1920x1080 frame (rng seed 0), "
+            "sample": f"{n} seeded rays of {what} (rng seed 0, {100.0 * n / scene.n_samples:.3g} %), "
                       f"{el:.1f} s on {threads} host threads"}
+
+
+def cpu_baseline_batch(scenes, target_s: float = 10.0) -> dict:
+    """The oracle on seeded rays drawn from 16 seeded scenes of a batch, the
+    same number from each, sized for about `target_s` seconds."""
+    import numpy as np
+    from oracle import oracle
+    rng = np.random.default_rng(0)
+    threads = len(os.sched_getaffinity(0))
+    pick = sorted(rng.choice(len(scenes), 16, replace=False).tolist())
+
+    def run(per):
+        t0 = time.perf_counter()
+        done = 0
+        for k in pick:
+            sc = scenes[k]
+            m = min(per, sc.n_samples)
+            idx = np.sort(rng.choice(sc.n_samples, m, replace=False)).astype(np.uint64)
+            oracle.trace_samples(sc, idx, threads=threads)
+            done += m
+        return done, time.perf_counter() - t0
+
+    n0, el0 = run(128)
+    per = int(max(128, 128 * target_s / max(el0, 1e-3)))
+    n, el = run(per)
+    return {"value": n / el, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{n} seeded rays, {per} from each of 16 seeded scenes of the batch "
+                      f"(rng seed 0), {el:.1f} s on {threads} host threads"}
 
 
 def run_ours(args) -> None:
@@ -424,6 +455,10 @@ def run_stress(args) -> None:
                                               "counts": hist}}
         cls_of[form] = cls
         del att
+    cpu = None
+    if not args.no_cpu_baseline:
+        cpu = cpu_baseline(workloads.kerr_stress_4k(side=side, spp=spp), 10.0,
+                           f"the {side}x{side}x{spp} spp frame")
     line = {"metric": "Kerr a=0.998 4096^2 x16 spp stress: geodesics/s and per-ray steps",
             "unit": UNIT, "n_gpus": 1, "higher_is_better": True,
             "config": {"workload": f"kerr_a0.998_{side}x{side}x{spp}spp_thin_disk",
@@ -435,6 +470,8 @@ def run_stress(args) -> None:
                                      / forms["fp64_dp45"]["geodesics_per_s"]),
             "class_agreement_mixed_vs_fp64_dp45":
                 float((cls_of["mixed"] == cls_of["fp64_dp45"]).double().mean())}
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
     r.close()
     print(json.dumps(line), flush=True)
 
@@ -507,6 +544,8 @@ def run_batch(args) -> None:
             "one_launch_per_scene": {"ms": single_ms, "geodesics_per_s": n / (single_ms * 1e-3)},
             "batch_over_one_launch_per_scene": single_ms / best}
     r.close()
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_batch(scenes)
     print(json.dumps(line), flush=True)
 
 

@@ -45,6 +45,15 @@ GG_CLASS_ESCAPED = 1
 GG_CLASS_DISK = 2
 GG_CLASS_MAXSTEPS = 3
 GG_CLASS_BUDGET = 4
+GG_CLASS_SCENE = 5
+GG_N_CLASSES = 6
+
+GG_PRIM_SPHERE = 0
+GG_PRIM_QUAD = 1
+GG_MAT_LAMBERTIAN = 0
+GG_MAT_DIFFUSE_LIGHT = 1
+GG_MAT_METAL = 2
+GG_MAT_DIELECTRIC = 3
 
 
 class gg_metric_t(C.Structure):
@@ -76,7 +85,7 @@ class gg_render_opts_t(C.Structure):
     _fields_ = [("samples_per_axis", C.c_uint32), ("jitter_spp", C.c_uint32),
                 ("seed", C.c_uint64), ("sky", C.c_int32), ("sky_rows", C.c_uint32),
                 ("sky_cols", C.c_uint32), ("row_offset", C.c_uint32), ("sky_seed", C.c_uint64),
-                ("attempt_budget", C.c_uint64), ("row_step", C.c_uint32), ("reserved", C.c_uint32)]
+                ("attempt_budget", C.c_uint64), ("row_step", C.c_uint32), ("scene", C.c_uint32)]
 
 
 class gg_ray_out_t(C.Structure):
@@ -94,8 +103,14 @@ class gg_scene_t(C.Structure):
 
 class gg_stats_t(C.Structure):
     _fields_ = [("rays", C.c_uint64), ("attempts", C.c_uint64), ("accepted", C.c_uint64),
-                ("class_count", C.c_uint64 * 5), ("kernel_ms", C.c_double),
+                ("class_count", C.c_uint64 * GG_N_CLASSES), ("kernel_ms", C.c_double),
                 ("fp64_rays", C.c_uint64), ("fp64_attempts", C.c_uint64)]
+
+
+class gg_prim_t(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("material", C.c_int32), ("p", C.c_double * 3),
+                ("u", C.c_double * 3), ("v", C.c_double * 3), ("radius", C.c_double),
+                ("color", C.c_double * 3), ("fuzz", C.c_double), ("ior", C.c_double)]
 
 
 STRUCTS = {
@@ -107,6 +122,7 @@ STRUCTS = {
     "gg_ray_out_t": gg_ray_out_t,
     "gg_scene_t": gg_scene_t,
     "gg_stats_t": gg_stats_t,
+    "gg_prim_t": gg_prim_t,
 }
 
 P = C.POINTER
@@ -147,6 +163,8 @@ _SIGNATURES = {
                                     P(gg_render_opts_t), P(C.c_int), P(C.c_double)]),
     "gg_batch_set_variant": (C.c_int, [C.c_void_p, C.c_int]),
     "gg_set_hdri": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_float]),
+    "gg_set_scene": (C.c_int, [C.c_void_p, P(gg_prim_t), C.c_uint32]),
+    "gg_scene_validate": (C.c_int, [P(gg_prim_t), C.c_uint32, P(C.c_uint32), P(C.c_uint32)]),
     "gg_forward_ckpt": (C.c_int, [C.c_void_p, P(gg_metric_t), C.c_double, C.c_double, C.c_double,
                                   C.c_double, P(gg_disk_t), P(gg_integrator_t),
                                   P(gg_render_opts_t), C.c_uint32, C.c_uint32, C.c_void_p,

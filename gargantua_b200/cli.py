@@ -8,10 +8,13 @@ hole, +z up, 60 degree FOV, aspect width / height), the same dispatch to
 reference's: ``Rendered WxH (metric[+disk]) in T s -> path``, where T runs
 from before the sky map is read until the PNG is written.
 
+``--scene lensed-spheres`` (main.rs:186-215) tests every step's chord
+against its five spheres on the GPU (render_with_scene, with ``--disk``
+render_with_disk_and_scene).
+
 Extensions: ``--precision mixed`` (the FP32/FP64 form, with the full
-Dormand-Prince stepper it needs), ``--device``.  ``--scene lensed-spheres``
-(the flat-space BVH scene of main.rs:186-215) is not on the GPU ray path and
-is refused with exit status 1, like an unknown scene.
+Dormand-Prince stepper it needs; not with ``--disk`` or a scene),
+``--device``.
 """
 from __future__ import annotations
 
@@ -25,6 +28,7 @@ from .curved import (AccretionDisk, Camera, HdriSky, ProceduralSky, RenderOption
                      Scene)
 from .gr_core import Kerr, RK45Integrator, Schwarzschild, renderer_integrator
 from .png import write_png
+from .workloads import lensed_spheres
 
 
 def parser() -> argparse.ArgumentParser:
@@ -59,8 +63,12 @@ def build_scene(args) -> Scene:
         metric = Kerr(args.mass, args.spin)
     else:
         raise ValueError(f"Unknown metric '{args.metric}'. Supported: schwarzschild, kerr")
-    if args.scene != "none":
-        raise ValueError(f"Unknown scene '{args.scene}'. Supported: none")
+    if args.scene == "none":
+        objects = None
+    elif args.scene == "lensed-spheres":
+        objects = lensed_spheres()
+    else:
+        raise ValueError(f"Unknown scene '{args.scene}'. Supported: none, lensed-spheres")
     sky = ProceduralSky()
     if args.hdri is not None:
         try:
@@ -76,7 +84,7 @@ def build_scene(args) -> Scene:
         opts.integrator = RK45Integrator(max_radius=base.max_radius, rtol=1e-8, atol=1e-10,
                                          stepper=abi.GG_STEPPER_DP45)
         opts.precision = abi.GG_PREC_MIXED
-    return Scene(metric, camera, args.width, args.height, disk, opts)
+    return Scene(metric, camera, args.width, args.height, disk, opts, objects)
 
 
 def main(argv=None, renderer: Renderer | None = None) -> int:
@@ -94,7 +102,7 @@ def main(argv=None, renderer: Renderer | None = None) -> int:
         print(f"render failed: {e}", file=sys.stderr)
         return 1
     write_png(args.output, img)
-    tags = ["disk"] if args.disk else []
+    tags = (["disk"] if args.disk else []) + ([args.scene] if args.scene != "none" else [])
     suffix = "+" + "+".join(tags) if tags else ""
     print(f"Rendered {args.width}x{args.height} ({args.metric}{suffix}) in "
           f"{time.perf_counter() - t0:.2f}s → {args.output}")

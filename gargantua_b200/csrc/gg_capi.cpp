@@ -12,11 +12,13 @@
 #include <cstring>
 #include <mutex>
 #include <new>
+#include <vector>
 
 #include "../../include/gargantua_gpu.h"
 #include "gg_host.h"
 #include "gg_launch.h"
 #include "gg_params.h"
+#include "gg_scene_host.h"
 
 using gg::DevControl;
 using gg::DevOutputs;
@@ -68,6 +70,12 @@ struct gg_ctx {
   size_t hdri_cap = 0;
   uint32_t hdri_w = 0, hdri_h = 0;
   float hdri_intensity = 1.f;
+  // scene of objects (gg_set_scene): primitives and hierarchy on the device
+  void* scene_prims = nullptr;
+  size_t scene_prims_cap = 0;
+  void* scene_nodes = nullptr;
+  size_t scene_nodes_cap = 0;
+  bool scene_set = false;
   bool pending = false;            // stats of the last device-pointer render not read yet
   gg_stats_t last{};
   std::mutex mu;
@@ -204,6 +212,7 @@ int validate(const gg_metric_t* metric, const gg_camera_t* camera, const gg_disk
     return GG_ERR_INVALID_ARG;
   if (opts->sky == GG_SKY_CHECKER && (opts->sky_rows < 1 || opts->sky_cols < 1))
     return GG_ERR_INVALID_ARG;
+  if (opts->scene > 1) return GG_ERR_INVALID_ARG;
   if (width < 1 || height < 1) return GG_ERR_INVALID_ARG;
   const uint64_t spa = opts->samples_per_axis < 1 ? 1 : opts->samples_per_axis;
   if (opts->jitter_spp == 0 && (spa * width > 0xffffffffull || spa * height > 0xffffffffull))
@@ -220,7 +229,13 @@ int validate(const gg_metric_t* metric, const gg_camera_t* camera, const gg_disk
 // positions by h*v_before, a first-order update whose endpoints follow the
 // exact step sequence, so FP32 rounding would show at 1e-4) with a thin disk
 // or none.
-int supported(const gg_disk_t* disk, const gg_integrator_t* integ) {
+int supported(const gg_disk_t* disk, const gg_integrator_t* integ,
+              const gg_render_opts_t* opts) {
+  // scene chords: the FP64 kernels, with no disk or the volumetric one (the
+  // reference's render_with_scene / render_with_disk_and_scene)
+  if (opts->scene &&
+      (integ->precision != GG_PREC_FP64 || (disk && disk->kind == GG_DISK_THIN)))
+    return GG_ERR_UNSUPPORTED;
   if (integ->precision == GG_PREC_MIXED) {
     if (integ->stepper != GG_STEPPER_DP45) return GG_ERR_UNSUPPORTED;
     if (disk && disk->kind == GG_DISK_VOLUMETRIC) return GG_ERR_UNSUPPORTED;
@@ -334,12 +349,18 @@ void build_params(const gg_metric_t* metric, const gg_camera_t* camera, const gg
   P.cell_h = kPi / (double)(opts->sky_rows ? opts->sky_rows : 1);
   P.cell_w = (2.0 * kPi) / (double)(opts->sky_cols ? opts->sky_cols : 1);
   P.attempt_budget = opts->attempt_budget;
+  P.scene = opts->scene;
   *out = P;
 }
 
 // The context's sky map into P for GG_SKY_HDRI renders; no map set is an
 // invalid argument.
 int attach_sky_map(const gg_ctx* c, DevParams* P) {
+  if (P->scene) {  // the context's scene, likewise
+    if (!c->scene_set) return GG_ERR_INVALID_ARG;
+    P->prims = static_cast<const gg::ScenePrim*>(c->scene_prims);
+    P->nodes = static_cast<const gg::SceneNode*>(c->scene_nodes);
+  }
   if (P->sky != gg::kSkyHdri) return GG_OK;
   if (!c->hdri) return GG_ERR_INVALID_ARG;
   P->hdri = c->hdri;
@@ -449,7 +470,7 @@ int collect(gg_ctx* ctx) {
   gg_stats_t s{};
   s.attempts = c.attempts;
   s.accepted = c.accepted;
-  for (int k = 0; k < 5; ++k) {
+  for (int k = 0; k < GG_N_CLASSES; ++k) {
     s.class_count[k] = c.class_count[k];
     s.rays += c.class_count[k];
   }
@@ -487,7 +508,7 @@ int batch_prepare(gg_ctx* c, const gg_scene_t* scenes, uint32_t n, const gg_inte
   if (integ->precision != GG_PREC_MIXED || integ->stepper != GG_STEPPER_DP45)
     return GG_ERR_UNSUPPORTED;
   if (opts->samples_per_axis > 1 || opts->jitter_spp > 0 || opts->attempt_budget != 0 ||
-      opts->row_step > 1 || opts->sky == GG_SKY_HDRI)
+      opts->row_step > 1 || opts->sky == GG_SKY_HDRI || opts->scene)
     return GG_ERR_UNSUPPORTED;
   const int kind = scenes[0].metric.kind, disk_kind = scenes[0].disk.kind;
   if (disk_kind != GG_DISK_NONE && disk_kind != GG_DISK_THIN) return GG_ERR_UNSUPPORTED;
@@ -675,6 +696,7 @@ GG_API int gg_struct_size(const char* name) {
            {"gg_ray_out_t", (int)sizeof(gg_ray_out_t)},
            {"gg_stats_t", (int)sizeof(gg_stats_t)},
            {"gg_scene_t", (int)sizeof(gg_scene_t)},
+           {"gg_prim_t", (int)sizeof(gg_prim_t)},
            // bytes that reach the device per render as kernel parameters
            {"launch_params", (int)(sizeof(DevParams) + sizeof(DevOutputs) + sizeof(void*))}};
   for (auto& e : t)
@@ -820,6 +842,8 @@ GG_API int gg_destroy(gg_ctx* c) {
   if (c->diff_grad) cudaFree(c->diff_grad);
   if (c->diff_grad_host) cudaFreeHost(c->diff_grad_host);
   if (c->hdri) cudaFree(c->hdri);
+  if (c->scene_prims) cudaFree(c->scene_prims);
+  if (c->scene_nodes) cudaFree(c->scene_nodes);
   if (c->ctl) cudaFree(c->ctl);
   if (c->ctl_host) cudaFreeHost(c->ctl_host);
   if (c->ev_start) cudaEventDestroy(c->ev_start);
@@ -854,7 +878,7 @@ GG_API int gg_render_device(gg_ctx* c, const gg_metric_t* metric, const gg_camer
   if (!c) return GG_ERR_INVALID_ARG;
   const int v = validate(metric, camera, disk, integ, opts, width, height);
   if (v != GG_OK) return v;
-  const int sup = supported(disk, integ);
+  const int sup = supported(disk, integ, opts);
   if (sup != GG_OK) return sup;
   DevParams P;
   build_params(metric, camera, disk, integ, opts, width, height, &P);
@@ -976,6 +1000,41 @@ GG_API int gg_set_hdri(gg_ctx* c, const float* rgb, uint32_t width, uint32_t hei
   return GG_OK;
 }
 
+GG_API int gg_set_scene(gg_ctx* c, const gg_prim_t* prims, uint32_t n) {
+  if (!c) return GG_ERR_INVALID_ARG;
+  std::vector<gg::ScenePrim> ps;
+  std::vector<gg::SceneNode> nodes;
+  if (n > 0) {
+    const int st = gg::build_scene(prims, n, &ps, &nodes, nullptr);
+    if (st != GG_OK) return st;
+  }
+  Lock lock(c);
+  // renders in flight may read the old scene
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return GG_ERR_CUDA;
+  if (cudaEventSynchronize(c->ev_done) != cudaSuccess) return GG_ERR_CUDA;
+  c->scene_set = false;
+  if (n == 0) return GG_OK;
+  const size_t pb = ps.size() * sizeof(gg::ScenePrim), nb = nodes.size() * sizeof(gg::SceneNode);
+  int st = grow(&c->scene_prims, &c->scene_prims_cap, pb);
+  if (st != GG_OK) return st;
+  st = grow(&c->scene_nodes, &c->scene_nodes_cap, nb);
+  if (st != GG_OK) return st;
+  if (cudaMemcpy(c->scene_prims, ps.data(), pb, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(c->scene_nodes, nodes.data(), nb, cudaMemcpyHostToDevice) != cudaSuccess)
+    return GG_ERR_CUDA;
+  c->scene_set = true;
+  return GG_OK;
+}
+
+GG_API int gg_scene_validate(const gg_prim_t* prims, uint32_t n, uint32_t* n_nodes,
+                             uint32_t* depth) {
+  std::vector<gg::ScenePrim> ps;
+  std::vector<gg::SceneNode> nodes;
+  const int st = gg::build_scene(prims, n, &ps, &nodes, depth);
+  if (st == GG_OK && n_nodes) *n_nodes = (uint32_t)nodes.size();
+  return st;
+}
+
 GG_API int gg_batch_set_variant(gg_ctx* c, int variant) {
   if (!c || variant < 0 || variant >= GG_BATCH_VARIANTS) return GG_ERR_INVALID_ARG;
   Lock lock(c);
@@ -997,7 +1056,7 @@ GG_API int gg_forward_ckpt(gg_ctx* c, const gg_metric_t* metric, double r_cam,
   if (metric->kind != GG_METRIC_KERR || disk->kind != GG_DISK_THIN ||
       integ->precision != GG_PREC_FP64 || integ->stepper != GG_STEPPER_DP45 ||
       opts->samples_per_axis > 1 || opts->jitter_spp > 0 || opts->attempt_budget != 0 ||
-      opts->row_step > 1 || opts->sky == GG_SKY_HDRI)
+      opts->row_step > 1 || opts->sky == GG_SKY_HDRI || opts->scene)
     return GG_ERR_UNSUPPORTED;
   Lock lock(c);
   DevParams P;
@@ -1060,7 +1119,7 @@ GG_API int gg_render(gg_ctx* c, const gg_metric_t* metric, const gg_camera_t* ca
   if (!c) return GG_ERR_INVALID_ARG;
   const int v = validate(metric, camera, disk, integ, opts, width, height);
   if (v != GG_OK) return v;
-  const int sup = supported(disk, integ);
+  const int sup = supported(disk, integ, opts);
   if (sup != GG_OK) return sup;
   DevParams P;
   build_params(metric, camera, disk, integ, opts, width, height, &P);

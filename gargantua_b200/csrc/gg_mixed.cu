@@ -371,7 +371,7 @@ __global__ void __launch_bounds__(kTraceBlock, MINB)
     atomicAdd(&ctl->attempts, bs.attempts);
     atomicAdd(&ctl->accepted, bs.accepted);
 #pragma unroll
-    for (int k = 0; k < 5; ++k)
+    for (int k = 0; k < kNumClasses; ++k)
       if (bs.cls[k]) atomicAdd(&ctl->class_count[k], bs.cls[k]);
   }
 }

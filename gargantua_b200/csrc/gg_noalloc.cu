@@ -69,7 +69,7 @@ extern "C" GG_API int gg_render_device_noalloc(const gg_metric_t* metric,
   const int v = gg::validate_render(metric, camera, disk, integ, opts, width, height);
   if (v != GG_OK) return v;
   if (integ->precision != GG_PREC_FP64 || opts->attempt_budget != 0 ||
-      opts->sky == GG_SKY_HDRI)  // the map belongs to a context
+      opts->sky == GG_SKY_HDRI || opts->scene)  // the map and scene belong to a context
     return GG_ERR_UNSUPPORTED;
   gg::DevParams P;
   gg::make_params(metric, camera, disk, integ, opts, width, height, &P);

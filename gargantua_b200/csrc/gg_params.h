@@ -15,7 +15,42 @@ namespace gg {
 enum : int { kMetricSchwarzschild = 0, kMetricKerr = 1 };
 enum : int { kDiskNone = 0, kDiskVolumetric = 1, kDiskThin = 2 };
 enum : int { kSkyProcedural = 0, kSkyChecker = 1, kSkyHdri = 2 };
-enum : int { kClsHorizon = 0, kClsEscaped = 1, kClsDisk = 2, kClsMaxSteps = 3, kClsBudget = 4 };
+enum : int {
+  kClsHorizon = 0,
+  kClsEscaped = 1,
+  kClsDisk = 2,
+  kClsMaxSteps = 3,
+  kClsBudget = 4,
+  kClsScene = 5,
+  kNumClasses = 6
+};
+
+// Scene primitive with the quantities its hit test and shading read,
+// prepared on the host: Sphere (sphere.rs:53-87), Quad (quad.rs:36-125,
+// with its precomputed unit normal, plane offset and e_alpha / e_beta).
+enum : int { kPrimSphere = 0, kPrimQuad = 1 };
+// shade_hit's albedo (tracer.rs:369-384): the material's scatter attenuation
+// when it scatters -- always (Lambertian, Dielectric: white), never
+// (DiffuseLight), or when the mirror direction leaves the surface (Metal
+// with fuzz 0).
+enum : int { kShadeAlbedo = 0, kShadeEmit = 1, kShadeMirror = 2 };
+struct ScenePrim {
+  int kind, shade;
+  double c[3];  // sphere centre / quad corner
+  double radius;
+  double n[3];  // quad unit normal
+  double d;     // quad plane offset n . Q
+  double ea[3], eb[3];
+  double albedo[3], emit[3];
+};
+// Bounding-volume hierarchy node: count > 0 is a leaf over prims
+// [first, first + count); count == 0 an inner node with children first and
+// first + 1.
+struct SceneNode {
+  double lo[3], hi[3];
+  int first, count;
+};
+constexpr int kSceneStack = 64;  // traversal stack; the host caps the depth below it
 enum : int { kStepperReference = 0, kStepperDP45 = 1 };
 
 struct DevParams {
@@ -68,6 +103,11 @@ struct DevParams {
   uint32_t hdri_w, hdri_h;
   float hdri_intensity;
   float pad_hdri;
+  // opts.scene: the context's scene, its hierarchy rooted at nodes[0]
+  const ScenePrim* prims;
+  const SceneNode* nodes;
+  uint32_t scene;
+  uint32_t pad_scene;
   // control
   uint64_t attempt_budget;
   double inv_spp;
@@ -146,7 +186,7 @@ struct DevControl {
   unsigned long long next_ray;   // work queue head
   unsigned long long attempts;   // step() calls, all rays
   unsigned long long accepted;
-  unsigned long long class_count[5];
+  unsigned long long class_count[kNumClasses];
   unsigned long long budget_used;
   unsigned int abort;            // set once the attempt budget is spent
   unsigned int queue_overflow;   // a mixed-form hand-off found the queue full

@@ -16,6 +16,7 @@
 
 #include "gg_device.cuh"
 #include "gg_launch.h"
+#include "gg_scene.cuh"
 #include "gg_trace_common.cuh"
 
 namespace gg {
@@ -26,8 +27,10 @@ namespace {
 // finishes, in FP64, the rays the mixed-precision pass handed over (their
 // count is read from ctl->queued, which that pass wrote before this launch).
 // BATCH (kSrcQueue only): the rays come from a batched render; each carries
-// its scene, whose parameters and outputs are in B.
-template <int METRIC, int DISK, int STEPPER, int SRC, bool BATCH>
+// its scene, whose parameters and outputs are in B.  SCENE (kSrcCamera, no
+// thin disk): every accepted step's chord is tested against P's scene of
+// objects first.
+template <int METRIC, int DISK, int STEPPER, int SRC, bool BATCH, bool SCENE>
 __global__ void __launch_bounds__(kTraceBlock,
                                   METRIC == kMetricKerr ? kTraceMinBlocksKerr : kTraceMinBlocksSchw)
     trace_fp64_kernel(const __grid_constant__ DevParams P, const __grid_constant__ DevOutputs O,
@@ -164,8 +167,33 @@ __global__ void __launch_bounds__(kTraceBlock,
       constexpr bool kSkyCross = STEPPER == kStepperDP45 && DISK != kDiskVolumetric;
       bool sky_at_cross = false;
       double sky_th = 0.0, sky_ph = 0.0;
+      double scene_rgb[3];
 
-      if (acc) {
+      if (SCENE && acc) {
+        // trace_ray_with_scene (tracer.rs:218-236): the chord between the
+        // step's ends, in Cartesian coordinates, against the scene
+        double cb[3], ca[3], dd[3];
+        sph_to_cart(xb, cb);
+        sph_to_cart(R.x, ca);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) dd[i] = sub_rn(ca[i], cb[i]);
+        if (dot3_nc(dd, dd) > 0.0) {
+          double t_hit;
+          const int k = scene_nearest(PL, cb, dd, t_hit);
+          if (k >= 0) {
+            scene_shade<METRIC>(PL, k, t_hit, cb, dd, scene_rgb);
+            if (DISK == kDiskVolumetric) {  // tracer.rs:293-309
+              double dl[3];
+              disk_color(inten, dl);
+#pragma unroll
+              for (int c = 0; c < 3; ++c) scene_rgb[c] = add_rn(mul_rn(scene_rgb[c], trans), dl[c]);
+            }
+            done_cls = kClsScene;
+          }
+        }
+      }
+
+      if (acc && done_cls < 0) {
         // The step's path: the reference's Euler segment (exactly linear in
         // the step fraction), or the full Dormand-Prince step's continuous
         // extension.
@@ -308,7 +336,14 @@ __global__ void __launch_bounds__(kTraceBlock,
         else if (res == kEscaped) done_cls = kClsEscaped;
         else if (n_att >= PL.max_steps) done_cls = kClsMaxSteps;
       }
-      if (done_cls >= 0) {
+      if (SCENE && done_cls == kClsScene) {
+        finish_scene_sample(PL, OL, idx, R, n_att, n_acc, inten, scene_rgb);
+        atomicAdd(&bs.attempts, (unsigned long long)n_att);
+        atomicAdd(&bs.accepted, (unsigned long long)n_acc);
+        atomicAdd(&bs.cls[kClsScene], 1ull);
+        budget_pending += n_att;
+        live = false;
+      } else if (done_cls >= 0) {
         finish(PL, OL, idx, done_cls, R, n_att, n_acc, out_int, out_temp, crossed,
                sky_at_cross ? sky_th : R.x[2], sky_at_cross ? sky_ph : R.x[3]);
         if (SRC == kSrcQueue) atomicAdd(&bs.fp64_att, (unsigned long long)(n_att - n_att0));
@@ -345,7 +380,7 @@ __global__ void __launch_bounds__(kTraceBlock,
     atomicAdd(&ctl->accepted, bs.accepted);
     if (SRC == kSrcQueue && bs.fp64_att) atomicAdd(&ctl->fp64_attempts, bs.fp64_att);
 #pragma unroll
-    for (int k = 0; k < 5; ++k)
+    for (int k = 0; k < kNumClasses; ++k)
       if (bs.cls[k]) atomicAdd(&ctl->class_count[k], bs.cls[k]);
   }
 }
@@ -368,13 +403,28 @@ __global__ void reduce_samples_kernel(const __grid_constant__ DevParams P, const
   }
 }
 
-template <int METRIC, int DISK, int STEPPER, int SRC, bool BATCH = false>
+template <int METRIC, int DISK, int STEPPER, int SRC, bool BATCH = false, bool SCENE = false>
 const void* trace_fn() {
-  return reinterpret_cast<const void*>(&trace_fp64_kernel<METRIC, DISK, STEPPER, SRC, BATCH>);
+  return reinterpret_cast<const void*>(
+      &trace_fp64_kernel<METRIC, DISK, STEPPER, SRC, BATCH, SCENE>);
+}
+
+// With a scene: no disk or the volumetric one (the reference's
+// render_with_scene and render_with_disk_and_scene).
+template <int STEPPER>
+const void* select_scene(const DevParams& P) {
+  if (P.metric == kMetricKerr)
+    return P.disk == kDiskVolumetric
+               ? trace_fn<kMetricKerr, kDiskVolumetric, STEPPER, kSrcCamera, false, true>()
+               : trace_fn<kMetricKerr, kDiskNone, STEPPER, kSrcCamera, false, true>();
+  return P.disk == kDiskVolumetric
+             ? trace_fn<kMetricSchwarzschild, kDiskVolumetric, STEPPER, kSrcCamera, false, true>()
+             : trace_fn<kMetricSchwarzschild, kDiskNone, STEPPER, kSrcCamera, false, true>();
 }
 
 template <int STEPPER>
 const void* select_metric_disk(const DevParams& P) {
+  if (P.scene) return select_scene<STEPPER>(P);
   if (P.metric == kMetricKerr) {
     if (P.disk == kDiskThin) return trace_fn<kMetricKerr, kDiskThin, STEPPER, kSrcCamera>();
     if (P.disk == kDiskVolumetric)

@@ -42,29 +42,11 @@ GG_DEV unsigned lanemask_lt() {
 // the hot stepping loop's instruction footprint.  (sky_th, sky_ph) is where
 // the checkerboard sky is read: the final position, or, for the full
 // Dormand-Prince stepper, the escape-sphere crossing.
-__device__ __noinline__ void finish_sample(const DevParams& P, const DevOutputs& O, uint64_t idx,
-                                           int cls, Ray R, uint32_t n_att, uint32_t n_acc,
-                                           double intensity, double color_temp, bool crossed,
-                                           double sky_th, double sky_ph) {
+GG_DEV void write_outcome(const DevParams& P, const DevOutputs& O, uint64_t idx, int cls,
+                          const Ray& R, uint32_t n_att, uint32_t n_acc, double intensity,
+                          double color_temp, bool crossed, const double lin[3]) {
   {
     const uint64_t n = P.n_rays;
-    double lin[3];
-    if (cls == kClsHorizon || cls == kClsBudget) {
-      lin[0] = lin[1] = lin[2] = 0.0;
-    } else if (cls == kClsEscaped) {
-      if (P.sky == kSkyChecker)
-        checker_sky(P, sky_th, sky_ph, lin);
-      else if (P.sky == kSkyHdri)
-        hdri_sky(P, R.v, lin);
-      else
-        procedural_sky(R.v, lin);
-    } else if (cls == kClsDisk) {
-      disk_color(intensity, lin);
-    } else {
-      lin[0] = 0.0;
-      lin[1] = 0.0;
-      lin[2] = 10.0 / 255.0;
-    }
     if (O.cls) O.cls[idx] = cls;
     if (O.x) {
 #pragma unroll
@@ -98,6 +80,40 @@ __device__ __noinline__ void finish_sample(const DevParams& P, const DevOutputs&
   }
 }
 
+__device__ __noinline__ void finish_sample(const DevParams& P, const DevOutputs& O, uint64_t idx,
+                                           int cls, Ray R, uint32_t n_att, uint32_t n_acc,
+                                           double intensity, double color_temp, bool crossed,
+                                           double sky_th, double sky_ph) {
+  double lin[3];
+  if (cls == kClsHorizon || cls == kClsBudget) {
+    lin[0] = lin[1] = lin[2] = 0.0;
+  } else if (cls == kClsEscaped) {
+    if (P.sky == kSkyChecker)
+      checker_sky(P, sky_th, sky_ph, lin);
+    else if (P.sky == kSkyHdri)
+      hdri_sky(P, R.v, lin);
+    else
+      procedural_sky(R.v, lin);
+  } else if (cls == kClsDisk) {
+    disk_color(intensity, lin);
+  } else {
+    lin[0] = 0.0;
+    lin[1] = 0.0;
+    lin[2] = 10.0 / 255.0;
+  }
+  write_outcome(P, O, idx, cls, R, n_att, n_acc, intensity, color_temp, crossed, lin);
+}
+
+// A ray whose chord hit the scene (RayOutcome::Scene): its colour was
+// shaded at the hit; `intensity` is the volumetric disk's up to the hit.
+__device__ __noinline__ void finish_scene_sample(const DevParams& P, const DevOutputs& O,
+                                                 uint64_t idx, Ray R, uint32_t n_att,
+                                                 uint32_t n_acc, double intensity,
+                                                 const double rgb[3]) {
+  const double lin[3] = {rgb[0], rgb[1], rgb[2]};
+  write_outcome(P, O, idx, kClsScene, R, n_att, n_acc, intensity, 0.0, false, lin);
+}
+
 // Camera ray of sample idx (once per ray, out of line like finish_sample).
 __device__ __noinline__ Ray start_sample(const DevParams& P, uint64_t idx) {
   double u, v;
@@ -111,7 +127,7 @@ __device__ __noinline__ Ray start_sample(const DevParams& P, uint64_t idx) {
 // ray instead of per-thread counters, which would cost registers in the
 // stepping loop); flushed to DevControl when the block exits.
 struct BlockStats {
-  unsigned long long attempts, accepted, cls[5], fp64_att;
+  unsigned long long attempts, accepted, cls[kNumClasses], fp64_att;
 };
 
 enum : int { kSrcCamera = 0, kSrcQueue = 1 };

@@ -7,6 +7,9 @@ run the CUDA library; there is no CPU path.
 
 ``HdriSky`` is the reference's equirectangular environment map
 (crates/raytracer/src/curved/sky.rs:43-123), sampled on the GPU.
+``render_with_scene`` / ``render_with_disk_and_scene`` (renderer.rs:110-254)
+test every step's chord against ``SceneObjects`` (spheres and quads) on the
+GPU.
 
 Extensions beyond the reference (all opt-in through ``RenderOptions`` or
 ``Scene``): a thin equatorial disk, a seeded checkerboard sky, seeded
@@ -160,6 +163,111 @@ class HdriSky:
 
 
 @dataclass
+class Lambertian:
+    """crates/raytracer/src/material/lambertian.rs: shaded with its albedo."""
+    albedo: tuple = (0.5, 0.5, 0.5)
+    kind = abi.GG_MAT_LAMBERTIAN
+
+    def color(self):
+        return self.albedo
+
+
+@dataclass
+class DiffuseLight:
+    """material/diffuse_light.rs: emits, does not scatter."""
+    emit: tuple = (1.0, 1.0, 1.0)
+    kind = abi.GG_MAT_DIFFUSE_LIGHT
+
+    def color(self):
+        return self.emit
+
+
+@dataclass
+class Metal:
+    """material/metal.rs; only fuzz = 0 renders (a fuzzed mirror's one-sample
+    shading depends on a random direction)."""
+    albedo: tuple = (0.8, 0.8, 0.8)
+    fuzz: float = 0.0
+    kind = abi.GG_MAT_METAL
+
+    def color(self):
+        return self.albedo
+
+
+@dataclass
+class Dielectric:
+    """material/dielectric.rs: always scatters, with white attenuation."""
+    ior: float = 1.5
+    kind = abi.GG_MAT_DIELECTRIC
+
+    def color(self):
+        return (1.0, 1.0, 1.0)
+
+
+@dataclass
+class Sphere:
+    """crates/raytracer/src/shape/sphere.rs:9-87."""
+    center: tuple
+    radius: float
+    material: object
+
+
+@dataclass
+class Quad:
+    """Parallelogram Q + a u + b v, a, b in [0, 1] (shape/quad.rs:8-125)."""
+    q: tuple
+    u: tuple
+    v: tuple
+    material: object
+
+
+class SceneObjects:
+    """A list of objects for the curved tracer, like ``World`` (scene/world.rs)
+    with ``add`` chaining; a Renderer uploads it (gg_set_scene, which builds
+    the bounding-volume hierarchy) the first time a render meets it, and
+    again after ``add``."""
+
+    def __init__(self, objects=()):
+        self.objects = []
+        self.version = 0
+        for o in objects:
+            self.add(o)
+
+    def add(self, obj) -> "SceneObjects":
+        if not isinstance(obj, (Sphere, Quad)):
+            raise TypeError("scene objects are Sphere or Quad")
+        self.objects.append(obj)
+        self.version += 1
+        return self
+
+    def __len__(self) -> int:
+        return len(self.objects)
+
+    def key(self):
+        return (id(self), self.version)
+
+    def to_c(self):
+        arr = (abi.gg_prim_t * len(self.objects))()
+        for k, o in enumerate(self.objects):
+            p = arr[k]
+            m = o.material
+            p.material = m.kind
+            p.color[:] = [float(x) for x in m.color()]
+            p.fuzz = float(getattr(m, "fuzz", 0.0))
+            p.ior = float(getattr(m, "ior", 0.0))
+            if isinstance(o, Sphere):
+                p.kind = abi.GG_PRIM_SPHERE
+                p.p[:] = [float(x) for x in o.center]
+                p.radius = float(o.radius)
+            else:
+                p.kind = abi.GG_PRIM_QUAD
+                p.p[:] = [float(x) for x in o.q]
+                p.u[:] = [float(x) for x in o.u]
+                p.v[:] = [float(x) for x in o.v]
+        return arr
+
+
+@dataclass
 class RenderOptions:
     """``RenderOptions`` (renderer.rs:17-26) plus the extensions listed above."""
 
@@ -204,6 +312,7 @@ class Scene:
     height: int
     disk: Union[AccretionDisk, ThinDisk, None] = None
     options: RenderOptions = field(default_factory=RenderOptions)
+    objects: Optional[SceneObjects] = None  # render_with_scene: chords against these
 
     @property
     def spp(self) -> int:
@@ -227,9 +336,10 @@ class Scene:
         return integ.to_c(self.options.max_steps, self.options.precision)
 
     def c_structs(self):
+        o = self.options.to_c()
+        o.scene = 1 if self.objects is not None else 0
         return (self.metric.to_c(), self.camera.to_c(),
-                self.disk.to_c() if self.disk is not None else None, self.integrator_c(),
-                self.options.to_c())
+                self.disk.to_c() if self.disk is not None else None, self.integrator_c(), o)
 
     def c_args(self):
         m, c, d, i, o = self.c_structs()
@@ -273,6 +383,7 @@ class Renderer:
         abi.check(self._lib.gg_create(C.byref(h), int(device)), "gg_create")
         self._h = h
         self._hdri_key = None
+        self._scene_key = None
 
     def close(self) -> None:
         if self._h:
@@ -300,10 +411,18 @@ class Renderer:
                                         px.shape[0], C.c_float(sky.intensity)), "gg_set_hdri")
         self._hdri_key = sky.key()
 
+    def set_scene(self, objects: SceneObjects) -> None:
+        """Uploads `objects` to this context (gg_set_scene)."""
+        arr = objects.to_c()
+        abi.check(self._lib.gg_set_scene(self._h, arr, len(arr)), "gg_set_scene")
+        self._scene_key = objects.key()
+
     def _sky_map(self, scene: Scene) -> None:
         sky = scene.options.sky
         if isinstance(sky, HdriSky) and sky.key() != self._hdri_key:
             self.set_hdri(sky)
+        if scene.objects is not None and scene.objects.key() != self._scene_key:
+            self.set_scene(scene.objects)
 
     def render(self, scene: Scene, rays: bool = False):
         """Synchronous render into host memory: (image, RayOutputs or None)."""
@@ -422,5 +541,22 @@ def render_with_disk(metric: Metric, camera: Camera, disk: Union[AccretionDisk, 
     return _renderer().render(scene)[0]
 
 
+def render_with_scene(metric: Metric, camera: Camera, objects: SceneObjects, width: int,
+                      height: int, opts: Optional[RenderOptions] = None) -> np.ndarray:
+    """``render_with_scene`` (renderer.rs:110-182)."""
+    scene = Scene(metric, camera, width, height, None, opts or RenderOptions(), objects)
+    return _renderer().render(scene)[0]
+
+
+def render_with_disk_and_scene(metric: Metric, camera: Camera, disk: AccretionDisk,
+                               objects: SceneObjects, width: int, height: int,
+                               opts: Optional[RenderOptions] = None) -> np.ndarray:
+    """``render_with_disk_and_scene`` (renderer.rs:184-254)."""
+    scene = Scene(metric, camera, width, height, disk, opts or RenderOptions(), objects)
+    return _renderer().render(scene)[0]
+
+
 __all__ = ["Camera", "AccretionDisk", "ThinDisk", "ProceduralSky", "CheckerSky", "HdriSky",
-           "RenderOptions", "Scene", "RayOutputs", "Renderer", "render", "render_with_disk"]
+           "Lambertian", "DiffuseLight", "Metal", "Dielectric", "Sphere", "Quad",
+           "SceneObjects", "RenderOptions", "Scene", "RayOutputs", "Renderer", "render",
+           "render_with_disk", "render_with_scene", "render_with_disk_and_scene"]

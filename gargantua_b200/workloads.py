@@ -12,13 +12,26 @@ from __future__ import annotations
 import math
 
 from . import abi
-from .curved import (AccretionDisk, Camera, CheckerSky, ProceduralSky, RenderOptions, Scene,
-                     ThinDisk)
+from .curved import (AccretionDisk, Camera, CheckerSky, DiffuseLight, Lambertian, ProceduralSky,
+                     RenderOptions, Scene, SceneObjects, Sphere, ThinDisk)
 from .gr_core import Kerr, RK45Integrator, Schwarzschild
 
 
 def disk_integrator(stepper: int = abi.GG_STEPPER_REFERENCE) -> RK45Integrator:
     return RK45Integrator(max_radius=200.0, rtol=1e-8, atol=1e-10, stepper=stepper)
+
+
+def lensed_spheres() -> SceneObjects:
+    """gr-renderer's ``--scene lensed-spheres`` (crates/gr-renderer/src/main.rs:186-215):
+    a luminous backdrop sphere behind the hole and four coloured Lambertian
+    spheres in a cross, 40-60 M out along the camera's line of sight."""
+    return SceneObjects([
+        Sphere((-60.0, 0.0, 0.0), 4.0, DiffuseLight((2.0, 1.6, 0.8))),
+        Sphere((-40.0, 14.0, 0.0), 3.5, Lambertian((0.85, 0.10, 0.10))),
+        Sphere((-40.0, -14.0, 0.0), 3.5, Lambertian((0.10, 0.75, 0.20))),
+        Sphere((-40.0, 0.0, 14.0), 3.5, Lambertian((0.15, 0.30, 0.90))),
+        Sphere((-40.0, 0.0, -14.0), 3.5, Lambertian((0.95, 0.85, 0.20))),
+    ])
 
 
 def reference_cli(width: int = 800, height: int = 600, metric: str = "schwarzschild",

@@ -134,7 +134,10 @@ typedef struct gg_render_opts_t {
    * share gets rows through the shadow); the image and per-sample outputs
    * then hold those rows only, in order.  0 or 1: every row. */
   uint32_t row_step;
-  uint32_t reserved;
+  /* 1: test every step's straight chord against the context's scene
+   * (gg_set_scene), render_with_scene / render_with_disk_and_scene
+   * (crates/raytracer/src/curved/renderer.rs:110-254); 0: no scene. */
+  uint32_t scene;
 } gg_render_opts_t;
 
 /* ---- per-sample outcome (RayOutcome + final GeodesicState) ------------- */
@@ -143,6 +146,8 @@ typedef struct gg_render_opts_t {
 #define GG_CLASS_DISK 2
 #define GG_CLASS_MAXSTEPS 3
 #define GG_CLASS_BUDGET 4 /* not traced: the attempt budget ran out         */
+#define GG_CLASS_SCENE 5  /* a step's chord hit the scene (RayOutcome::Scene) */
+#define GG_N_CLASSES 6
 
 /* Every pointer is optional (NULL: not written).  Arrays have one entry per
  * sample, ordered sample-major inside a pixel and pixels row-major:
@@ -169,7 +174,7 @@ typedef struct gg_stats_t {
   uint64_t rays;
   uint64_t attempts;
   uint64_t accepted;
-  uint64_t class_count[5];
+  uint64_t class_count[GG_N_CLASSES];
   double kernel_ms; /* device time of the trace launch(es)                 */
   /* GG_PREC_MIXED: rays the FP32 pass handed to the FP64 pass (FP64 band)
    * and the attempts made in that pass; 0 for GG_PREC_FP64 */
@@ -337,6 +342,45 @@ GG_API int gg_backward(gg_ctx* ctx, const double* dl_drgb_dev, double grad[5], v
  * in y) at the escape direction, scaled by `intensity`. */
 GG_API int gg_set_hdri(gg_ctx* ctx, const float* rgb, uint32_t width, uint32_t height,
                        float intensity);
+
+/* ---- scene of objects in the spatial slice ----------------------------- */
+/* raytracer::shape::{Sphere, Quad} (crates/raytracer/src/shape/sphere.rs:9-87,
+ * quad.rs:8-125) with the materials whose one-sample shading the curved
+ * tracer's shade_hit (curved/tracer.rs:369-384) reads deterministically:
+ * Lambertian (albedo), DiffuseLight (emission), Metal with fuzz 0 (albedo
+ * when the mirror direction leaves the surface) and Dielectric (white).
+ * Coordinates are the Cartesian image of Boyer-Lindquist (r, theta, phi):
+ * (r sin th cos ph, r sin th sin ph, r cos th). */
+#define GG_PRIM_SPHERE 0
+#define GG_PRIM_QUAD 1
+#define GG_MAT_LAMBERTIAN 0
+#define GG_MAT_DIFFUSE_LIGHT 1
+#define GG_MAT_METAL 2
+#define GG_MAT_DIELECTRIC 3
+
+typedef struct gg_prim_t {
+  int32_t kind;      /* GG_PRIM_*                                          */
+  int32_t material;  /* GG_MAT_*                                           */
+  double p[3];       /* sphere centre, or quad corner Q                    */
+  double u[3];       /* quad edge u                                        */
+  double v[3];       /* quad edge v                                        */
+  double radius;     /* sphere radius (> 0)                                */
+  double color[3];   /* albedo (Lambertian, Metal) or emission (DiffuseLight) */
+  double fuzz;       /* Metal: 0 (a fuzzed mirror samples a random direction) */
+  double ior;        /* Dielectric index of refraction (shading ignores it) */
+} gg_prim_t;
+
+/* Sets the context's scene (copied; a bounding-volume hierarchy is built
+ * over it).  n = 0 clears it.  Renders with opts.scene = 1 test each
+ * accepted step's chord against it; rays whose chord hits end with
+ * GG_CLASS_SCENE and the shaded, redshifted surface colour. */
+GG_API int gg_set_scene(gg_ctx* ctx, const gg_prim_t* prims, uint32_t n);
+
+/* The checks and hierarchy build of gg_set_scene without a device: GG_OK
+ * (and, when not NULL, the hierarchy's node count and depth) or the error
+ * gg_set_scene would return. */
+GG_API int gg_scene_validate(const gg_prim_t* prims, uint32_t n, uint32_t* n_nodes,
+                             uint32_t* depth);
 
 /* ---- measurement ------------------------------------------------------- */
 /* FMA throughput of the context's device in FLOP/s (an FMA counts 2), best

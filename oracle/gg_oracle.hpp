@@ -26,6 +26,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <vector>
 
 namespace ggo {
 
@@ -1040,6 +1041,166 @@ inline void hdri_sky(const HdriMap& m, const V3& dir, double rgb[3]) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Objects in the spatial slice (render_with_scene).
+// ---------------------------------------------------------------------------
+enum ObjKind { kObjSphere = 0, kObjQuad = 1 };
+enum MatKind { kMatLambertian = 0, kMatDiffuseLight = 1, kMatMetal = 2, kMatDielectric = 3 };
+
+struct SceneObj {
+  int kind = kObjSphere, material = kMatLambertian;
+  V3 center{}, q{}, u{}, v{};
+  double radius = 1.0;
+  V3 color{};  // Lambertian / Metal albedo, DiffuseLight emission
+  // Quad::with_arc_material (quad.rs:36-79)
+  V3 normal{}, e_alpha{}, e_beta{};
+  double d = 0.0;
+};
+
+inline V3 sub3(const V3& a, const V3& b) { return {{a[0] - b[0], a[1] - b[1], a[2] - b[2]}}; }
+
+inline SceneObj make_quad(const V3& q, const V3& u, const V3& v, int material, const V3& color) {
+  SceneObj o;
+  o.kind = kObjQuad;
+  o.material = material;
+  o.q = q;
+  o.u = u;
+  o.v = v;
+  o.color = color;
+  V3 n = cross(u, v);
+  o.normal = normalize(n);
+  o.d = dot(o.normal, q);
+  double nn = dot(n, n);
+  V3 w{{n[0] / nn, n[1] / nn, n[2] / nn}};
+  o.e_alpha = cross(v, w);
+  o.e_beta = cross(w, u);
+  return o;
+}
+
+struct Hit {
+  double t = 0.0;
+  V3 point{}, normal{};
+  bool front_face = false;
+  const SceneObj* obj = nullptr;
+};
+
+// HitRecord::new (core/hit.rs): the normal faces the incoming ray
+inline void set_face(Hit& h, const V3& dir, const V3& outward) {
+  h.front_face = dot(dir, outward) < 0.0;
+  h.normal = h.front_face ? outward : V3{{-outward[0], -outward[1], -outward[2]}};
+}
+
+// Sphere::hit (sphere.rs:53-87)
+inline bool sphere_hit(const SceneObj& s, const V3& o, const V3& dir, double t_min, double t_max,
+                       Hit& h) {
+  V3 oc = sub3(o, s.center);
+  double a = dot(dir, dir);
+  double half_b = dot(oc, dir);
+  double c = dot(oc, oc) - s.radius * s.radius;
+  double disc = half_b * half_b - a * c;
+  if (disc < 0.0) return false;
+  double sq = std::sqrt(disc);
+  double root = (-half_b - sq) / a;
+  if (!(t_min < root && root < t_max)) {
+    root = (-half_b + sq) / a;
+    if (!(t_min < root && root < t_max)) return false;
+  }
+  h.t = root;
+  h.point = o + root * dir;
+  V3 diff = sub3(h.point, s.center);
+  set_face(h, dir, V3{{diff[0] / s.radius, diff[1] / s.radius, diff[2] / s.radius}});
+  h.obj = &s;
+  return true;
+}
+
+// Quad::hit (quad.rs:85-125)
+inline bool quad_hit(const SceneObj& s, const V3& o, const V3& dir, double t_min, double t_max,
+                     Hit& h) {
+  double denom = dot(s.normal, dir);
+  if (std::fabs(denom) < 1e-8) return false;
+  double t = (s.d - dot(s.normal, o)) / denom;
+  if (!(t_min < t && t < t_max)) return false;
+  V3 p = o + t * dir;
+  V3 planar = sub3(p, s.q);
+  double alpha = dot(planar, s.e_alpha);
+  double beta = dot(planar, s.e_beta);
+  if (alpha < 0.0 || alpha > 1.0 || beta < 0.0 || beta > 1.0) return false;
+  h.t = t;
+  h.point = p;
+  set_face(h, dir, s.normal);
+  h.obj = &s;
+  return true;
+}
+
+// The nearest hit over all objects for t in (t_min, t_max): what
+// World::hit (scene/world.rs:69-81) and BvhNode::hit (accel/bvh.rs:184-254)
+// both return, the upper bound shrinking to each hit found.
+inline bool scene_hit(const std::vector<SceneObj>& objs, const V3& o, const V3& dir,
+                      double t_min, double t_max, Hit& best) {
+  bool any = false;
+  for (const SceneObj& s : objs) {
+    Hit h;
+    bool hit = s.kind == kObjSphere ? sphere_hit(s, o, dir, t_min, t_max, h)
+                                    : quad_hit(s, o, dir, t_min, t_max, h);
+    if (hit) {
+      best = h;
+      t_max = h.t;
+      any = true;
+    }
+  }
+  return any;
+}
+
+// shade_hit (curved/tracer.rs:369-384) with the material's scatter
+// attenuation: Lambertian albedo (lambertian.rs:42-56), DiffuseLight none
+// (diffuse_light.rs:22-30), Metal with fuzz 0 its albedo when the mirror
+// direction leaves the surface (metal.rs:40-57, reflect :109-111),
+// Dielectric white (dielectric.rs:65-95); emission from DiffuseLight only.
+inline void shade_hit(const V3& dir, const Hit& h, double lin[3]) {
+  const SceneObj& s = *h.obj;
+  V3 albedo{{0.0, 0.0, 0.0}}, emission{{0.0, 0.0, 0.0}};
+  V3 unit = normalize(dir);
+  switch (s.material) {
+    case kMatLambertian: albedo = s.color; break;
+    case kMatDiffuseLight: emission = s.color; break;
+    case kMatMetal: {
+      double two_dot = 2.0 * dot(unit, h.normal);
+      V3 refl = sub3(unit, two_dot * h.normal);
+      if (dot(refl, h.normal) > 0.0) albedo = s.color;
+      break;
+    }
+    default: albedo = V3{{1.0, 1.0, 1.0}}; break;
+  }
+  V3 neg{{-unit[0], -unit[1], -unit[2]}};
+  double nd = rmax(dot(neg, h.normal), 0.0);
+  double facing = 0.5 + 0.5 * nd;
+  for (int c = 0; c < 3; ++c) lin[c] = albedo[c] * facing + emission[c];
+}
+
+// spherical_to_cartesian / cartesian_to_spherical (curved/tracer.rs:11-28)
+inline V3 spherical_to_cartesian(const V4<double>& p) {
+  double r = p[1], theta = p[2], phi = p[3];
+  double st = std::sin(theta);
+  return {{r * st * std::cos(phi), r * st * std::sin(phi), r * std::cos(theta)}};
+}
+inline V4<double> cartesian_to_spherical(const V3& p) {
+  double r = rmax(std::sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]), 1e-10);
+  double z = p[2] / r;
+  if (z < -1.0) z = -1.0;
+  if (z > 1.0) z = 1.0;
+  return {{0.0, r, std::acos(z), std::atan2(p[1], p[0])}};
+}
+
+// redshift_g4_static (curved/tracer.rs:40-52)
+template <class M>
+double redshift_g4_static(const M& metric, const V4<double>& pos_emit, double g_tt_obs) {
+  double g_tt_emit = -metric.metric_tensor(pos_emit).tt;
+  if (g_tt_emit <= 0.0 || g_tt_obs <= 0.0) return 0.0;
+  double g = std::sqrt(g_tt_emit / g_tt_obs);
+  double g2 = g * g;
+  return g2 * g2;
+}
+
 inline void disk_color(double intensity, double rgb[3]) {  // renderer.rs:62-66
   double x = intensity / (1.0 + intensity);
   rgb[0] = std::pow(x, 0.5);
@@ -1060,7 +1221,7 @@ inline uint8_t encode_channel(double c) {  // renderer.rs:69-80
 // ---------------------------------------------------------------------------
 // Tracing one sample.
 // ---------------------------------------------------------------------------
-enum RayClass { kClsHorizon = 0, kClsEscaped = 1, kClsDisk = 2, kClsMaxSteps = 3 };
+enum RayClass { kClsHorizon = 0, kClsEscaped = 1, kClsDisk = 2, kClsMaxSteps = 3, kClsScene = 5 };
 enum DiskKind { kDiskNone = 0, kDiskVolumetric = 1, kDiskThin = 2 };
 enum SkyKind { kSkyProcedural = 0, kSkyChecker = 1, kSkyHdri = 2 };
 
@@ -1078,6 +1239,7 @@ struct TraceSetup {
   uint32_t sky_rows = 18, sky_cols = 36;
   uint64_t sky_seed = 0;
   HdriMap hdri;
+  const std::vector<SceneObj>* scene = nullptr;  // render_with_scene when set
 };
 
 struct Sample {
@@ -1087,6 +1249,7 @@ struct Sample {
   double intensity = 0.0, color_temp = 0.0;
   double cross[8];  // state at the escape sphere / disk plane, NaN otherwise
   double rgb[3] = {0, 0, 0};
+  double scene_rgb[3] = {0, 0, 0};  // RayOutcome::Scene colour
 };
 
 inline void fill_nan(double* p, int n) {
@@ -1126,6 +1289,9 @@ void shade(const M&, const TraceSetup& S, Sample& o) {  // renderer.rs:44-53
       }
       break;
     case kClsDisk: disk_color(o.intensity, o.rgb); break;
+    case kClsScene:
+      for (int c = 0; c < 3; ++c) o.rgb[c] = o.scene_rgb[c];
+      break;
     default: o.rgb[0] = 0.0; o.rgb[1] = 0.0; o.rgb[2] = 10.0 / 255.0; break;
   }
 }
@@ -1160,6 +1326,31 @@ Sample trace(const M& metric, const TraceSetup& S, const V4<double>& observer,
     StepResult result = S.integ.step(metric, st, h, &acc, &h_used, ends);
     o.attempts += 1;
     if (acc) o.accepted += 1;
+    if (S.scene) {
+      // trace_ray_with_scene (tracer.rs:218-236) / trace_ray_with_disk_and_scene
+      // (:279-310): the step's Cartesian chord against the scene, before the
+      // disk; a step that did not move has no chord
+      V3 cb = spherical_to_cartesian(before.position);
+      V3 ca = spherical_to_cartesian(st.position);
+      V3 seg = sub3(ca, cb);
+      if (norm(seg) > 0.0) {
+        Hit hit;
+        if (scene_hit(*S.scene, cb, seg, 0.0, 1.0, hit)) {
+          double lin[3];
+          shade_hit(seg, hit, lin);
+          double g4 = redshift_g4_static(metric, cartesian_to_spherical(hit.point), g_tt_obs);
+          if (S.disk_kind == kDiskVolumetric) {
+            double dl[3];
+            disk_color(intensity, dl);
+            for (int c = 0; c < 3; ++c) o.scene_rgb[c] = lin[c] * g4 * transmission + dl[c];
+          } else {
+            for (int c = 0; c < 3; ++c) o.scene_rgb[c] = lin[c] * g4;
+          }
+          o.intensity = intensity;
+          return finish(kClsScene);
+        }
+      }
+    }
     if (acc) {
       const bool dp45 = S.integ.stepper == 1;
       const double dl = h_used;

@@ -48,6 +48,8 @@ RK45 make_rk45(const gg_integrator_t* in) {
 // The sky map GG_SKY_HDRI renders sample (ggo_set_hdri); one per process.
 std::vector<float> g_hdri_px;
 HdriMap g_hdri;
+// The objects of opts.scene renders (ggo_set_scene); one per process.
+std::vector<SceneObj> g_scene;
 
 TraceSetup make_setup(const gg_disk_t* disk, const gg_integrator_t* integ,
                       const gg_render_opts_t* opts) {
@@ -70,6 +72,7 @@ TraceSetup make_setup(const gg_disk_t* disk, const gg_integrator_t* integ,
   S.sky_cols = opts->sky_cols;
   S.sky_seed = opts->sky_seed;
   S.hdri = g_hdri;
+  if (opts->scene) S.scene = &g_scene;
   return S;
 }
 
@@ -424,6 +427,46 @@ GGO_API int ggo_set_hdri(const float* rgb, uint32_t width, uint32_t height, floa
   g_hdri.height = height;
   g_hdri.intensity = intensity;
   return 0;
+}
+
+// Sets the objects of opts.scene renders: spheres and quads with Lambertian,
+// DiffuseLight, Metal (fuzz 0) or Dielectric materials.  Returns 0, or -1
+// for an unknown kind or material.
+GGO_API int ggo_set_scene(const gg_prim_t* prims, uint32_t n) {
+  std::vector<SceneObj> objs;
+  for (uint32_t k = 0; k < n; ++k) {
+    const gg_prim_t& p = prims[k];
+    if (p.material < kMatLambertian || p.material > kMatDielectric) return -1;
+    V3 a{{p.p[0], p.p[1], p.p[2]}}, color{{p.color[0], p.color[1], p.color[2]}};
+    if (p.kind == kObjSphere) {
+      SceneObj o;
+      o.kind = kObjSphere;
+      o.material = p.material;
+      o.center = a;
+      o.radius = p.radius;
+      o.color = color;
+      objs.push_back(o);
+    } else if (p.kind == kObjQuad) {
+      objs.push_back(make_quad(a, V3{{p.u[0], p.u[1], p.u[2]}}, V3{{p.v[0], p.v[1], p.v[2]}},
+                               p.material, color));
+    } else {
+      return -1;
+    }
+  }
+  g_scene = std::move(objs);
+  return 0;
+}
+
+// The nearest hit of the chord o + t d, t in (0, 1), over the objects set by
+// ggo_set_scene: returns the object's index or -1, with t and the shaded
+// (unredshifted) colour.
+GGO_API int ggo_scene_hit(const double o[3], const double d[3], double* t, double rgb[3]) {
+  Hit h;
+  V3 dir{{d[0], d[1], d[2]}};
+  if (!scene_hit(g_scene, V3{{o[0], o[1], o[2]}}, dir, 0.0, 1.0, h)) return -1;
+  *t = h.t;
+  shade_hit(dir, h, rgb);
+  return (int)(h.obj - g_scene.data());
 }
 
 // HdriSky::sample of the map set by ggo_set_hdri at direction dir.

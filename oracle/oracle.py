@@ -82,6 +82,8 @@ def lib(variant: str = "plain") -> C.CDLL:
             "ggo_disk_color": (None, [C.c_double, C.c_void_p]),
             "ggo_set_hdri": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_float]),
             "ggo_hdri_sky": (None, [C.c_void_p, C.c_void_p]),
+            "ggo_set_scene": (C.c_int, [P(abi.gg_prim_t), C.c_uint32]),
+            "ggo_scene_hit": (C.c_int, [C.c_void_p, C.c_void_p, P(C.c_double), C.c_void_p]),
             "ggo_encode_srgb": (None, [C.c_void_p, C.c_void_p]),
             "ggo_splitmix64": (C.c_uint64, [C.c_uint64]),
             "ggo_sample_uv": (None, [P(abi.gg_render_opts_t), C.c_uint32, C.c_uint32,
@@ -120,10 +122,30 @@ def hdri_sample(sky, direction) -> np.ndarray:
     return out
 
 
+def set_objects(objects, variant: str = "plain") -> None:
+    """Makes `objects` (gargantua_b200.curved.SceneObjects) the scene of opts.scene renders."""
+    arr = objects.to_c()
+    if lib(variant).ggo_set_scene(arr, len(arr)):
+        raise ValueError("unknown primitive kind or material")
+
+
+def scene_hit(objects, origin, direction):
+    """(index or -1, t, shaded colour) of the chord origin + t direction, t in (0, 1)."""
+    set_objects(objects)
+    o = np.ascontiguousarray(origin, np.float64)
+    d = np.ascontiguousarray(direction, np.float64)
+    t = C.c_double(0.0)
+    rgb = np.zeros(3)
+    k = lib().ggo_scene_hit(_ptr(o), _ptr(d), C.byref(t), _ptr(rgb))
+    return k, t.value, rgb
+
+
 def _sky_map(scene, variant: str) -> None:
     from gargantua_b200.curved import HdriSky
     if isinstance(scene.options.sky, HdriSky):
         set_hdri(scene.options.sky, variant)
+    if scene.objects is not None:
+        set_objects(scene.objects, variant)
 
 
 def render(scene, threads: int = 0, rays: bool = True, variant: str = "plain"):

@@ -57,7 +57,7 @@ def test_scene_of_arguments(tmp_path):
 
 
 @pytest.mark.parametrize("argv", [["--metric", "minkowski"], ["--scene", "teapot"],
-                                  ["--scene", "lensed-spheres"], ["--hdri", "/nonexistent.hdr"]])
+                                  ["--hdri", "/nonexistent.hdr"]])
 def test_bad_arguments_exit_1(argv, capsys, tmp_path):
     assert cli.main(argv + ["--output", str(tmp_path / "x.png")]) == 1
     assert capsys.readouterr().err

@@ -249,7 +249,9 @@ def test_map_kerr_volumetric(renderer, oracle_mod):
     scene = workloads.schwarzschild_thin_256()
     scene.metric = Kerr(1.0, 0.6)
     from gargantua_b200.curved import AccretionDisk
-    scene.disk = AccretionDisk()
+    # the density is nonzero on the whole cylindrical shell r_in <= R <= r_out
+    # at any height, so only rays passing outside R = 8 M escape
+    scene.disk = AccretionDisk(r_inner=6.0, r_outer=8.0)
     scene.width = scene.height = 96
     _with_sky(scene, sky)
     _, g = renderer.render(scene, rays=True)
