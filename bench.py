@@ -365,8 +365,10 @@ def run_ours(args) -> None:
         "e2e": {"value": H["full"].n_samples * steps / e2e_s, "unit": UNIT,
                 "h2d_bytes_per_step": abi.load().gg_struct_size(b"launch_params"),
                 "d2h_bytes_per_step": scene.width * scene.rows * 3},
-        # per step: the mixed kernel and the FP64 band pass
-        "gpu_launches": 2 * steps,
+        # per step: the mixed kernel, the FP64 band pass (which hands rays
+        # clear of the band back), the round reset, the mixed pass over the
+        # returned rays and the last FP64 pass
+        "gpu_launches": 5 * steps,
         "roofline": {"bound": "fp32", "achieved": achieved / 1e12,
                      "peak": peak / 1e12, "unit": "TFLOP/s", "frac": achieved / peak,
                      "traffic": None,

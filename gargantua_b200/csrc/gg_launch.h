@@ -39,15 +39,19 @@ cudaError_t launch_trace(const DevParams& P, const DevOutputs& O, DevControl* ct
 
 // Mixed form (P.precision == GG_PREC_MIXED, full Dormand-Prince): the FP32
 // pass over the samples, which hands FP64-band rays to O.queue, and the FP64
-// pass over that queue.
+// pass over that queue, which (P.hand_back) returns rays clear of the band to
+// O.ret; then, after launch_next_round, the FP32 pass over O.ret (`returned`)
+// and a last FP64 pass without hand-back.
 // A batched render (batch != nullptr) runs one of kBatchVariants kernel
 // variants (compaction period x register budget), chosen by `variant`.
 constexpr int kBatchVariants = 6;
 cudaError_t mixed_occupancy(const DevParams& P, int* blocks_per_sm,
-                            const BatchTable* batch = nullptr, int variant = 0);
+                            const BatchTable* batch = nullptr, int variant = 0,
+                            bool returned = false);
 cudaError_t launch_mixed(const DevParams& P, const DevOutputs& O, DevControl* ctl, int grid,
                          cudaStream_t stream, const BatchTable* batch = nullptr,
-                         int variant = 0);
+                         int variant = 0, bool returned = false);
+cudaError_t launch_next_round(DevControl* ctl, cudaStream_t stream);
 cudaError_t queue_trace_occupancy(const DevParams& P, int* blocks_per_sm);
 cudaError_t launch_queue_trace(const DevParams& P, const DevOutputs& O, DevControl* ctl,
                                int grid, cudaStream_t stream,

@@ -181,7 +181,9 @@ constexpr uint32_t kPendClsShift = 8;                  // kPendFinish: the class
 // (the integrator, sky kind and budget are the batch's, in P).  PERIOD
 // (attempts between refills) and MINB (CTAs per SM the registers are
 // budgeted for) are the settings the batch autotuner chooses between.
-template <int METRIC, int DISK, bool BUDGET, bool BATCH, int PERIOD, int MINB>
+// SRC: kSrcCamera starts the samples from the camera; kSrcQueue continues the
+// rays the FP64 pass handed back (O.ret, ctl->returned of them).
+template <int METRIC, int DISK, bool BUDGET, bool BATCH, int PERIOD, int MINB, int SRC>
 __global__ void __launch_bounds__(kTraceBlock, MINB)
     trace_mixed_kernel(const __grid_constant__ DevParams P, const __grid_constant__ DevOutputs O,
                        DevControl* ctl, const __grid_constant__ BatchTable B) {
@@ -212,6 +214,9 @@ __global__ void __launch_bounds__(kTraceBlock, MINB)
   uint32_t wcount = 0;
   bool wdone = false;
   unsigned budget_pending = 0;
+  const uint64_t n_src =
+      SRC == kSrcQueue ? (ctl->returned < O.ret_cap ? ctl->returned : O.ret_cap) : P.n_rays;
+  unsigned long long* const head = SRC == kSrcQueue ? &ctl->next_returned : &ctl->next_ray;
 
   for (;;) {
     // ---- deferred per-ray work ---------------------------------------------
@@ -253,37 +258,53 @@ __global__ void __launch_bounds__(kTraceBlock, MINB)
       if (wcount == 0) {
         unsigned long long b = 0;
         if (lane == 0) {
-          b = atomicAdd(&ctl->next_ray, (unsigned long long)kChunk);
+          b = atomicAdd(head, (unsigned long long)kChunk);
           if (BUDGET) {
             const unsigned long long used = atomicAdd(&ctl->budget_used, 0ull);
             if (used > P.attempt_budget) {
               atomicExch(&ctl->abort, 1u);
-              b = P.n_rays;
+              b = n_src;
             }
           }
         }
         b = __shfl_sync(kFull, b, 0);
-        if (b >= P.n_rays) {
+        if (b >= n_src) {
           wdone = true;
           break;
         }
         wbase = b;
-        const uint64_t left = P.n_rays - b;
+        const uint64_t left = n_src - b;
         wcount = left < kChunk ? (uint32_t)left : kChunk;
       }
       const unsigned nn = (unsigned)__popc(need);
       const unsigned take = nn < wcount ? nn : wcount;
       const unsigned rank = (unsigned)__popc(need & lanemask_lt());
       if (!live && rank < take) {
-        uint64_t idx = wbase + rank;
-        if (BATCH) {
-          scene = find_scene(B, idx);
-          idx -= B.first[scene];
+        if (SRC == kSrcQueue) {
+          const QueuedRay& q = O.ret[wbase + rank];
+          Ray R;
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            R.x[i] = q.x[i];
+            R.v[i] = q.v[i];
+          }
+          R.h = q.h;
+          R.lam = q.lam;
+          if (BATCH) scene = q.scene;
+          mixed_load(R, q.idx, K, S);
+          n_att = q.n_att;
+          n_acc = q.n_acc;
+        } else {
+          uint64_t idx = wbase + rank;
+          if (BATCH) {
+            scene = find_scene(B, idx);
+            idx -= B.first[scene];
+          }
+          mixed_load(start_sample(BATCH ? B.scenes[scene].P : P, idx), idx, K, S);
+          n_att = 0;
+          n_acc = 0;
         }
-        mixed_load(start_sample(BATCH ? B.scenes[scene].P : P, idx), idx, K, S);
         live = true;
-        n_att = 0;
-        n_acc = 0;
         crossed = false;
         k1_valid = false;
         k7_pending = false;
@@ -377,10 +398,10 @@ __global__ void __launch_bounds__(kTraceBlock, MINB)
 }
 
 template <int METRIC, int DISK, bool BUDGET, bool BATCH = false, int PERIOD = kMixedPeriod,
-          int MINB = kMixedMinBlocks>
+          int MINB = kMixedMinBlocks, int SRC = kSrcCamera>
 const void* mixed_fn() {
   return reinterpret_cast<const void*>(
-      &trace_mixed_kernel<METRIC, DISK, BUDGET, BATCH, PERIOD, MINB>);
+      &trace_mixed_kernel<METRIC, DISK, BUDGET, BATCH, PERIOD, MINB, SRC>);
 }
 
 template <bool BUDGET>
@@ -390,6 +411,20 @@ const void* select_mixed_disk(const DevParams& P) {
                                : mixed_fn<kMetricKerr, kDiskNone, BUDGET>();
   return P.disk == kDiskThin ? mixed_fn<kMetricSchwarzschild, kDiskThin, BUDGET>()
                              : mixed_fn<kMetricSchwarzschild, kDiskNone, BUDGET>();
+}
+
+// The pass over the rays the FP64 pass handed back (no attempt budget: the
+// hand-back is off in budgeted renders).
+template <bool BATCH>
+const void* select_returned(const DevParams& P) {
+  constexpr int Pd = kMixedPeriod, Mb = kMixedMinBlocks;
+  if (P.metric == kMetricKerr)
+    return P.disk == kDiskThin
+               ? mixed_fn<kMetricKerr, kDiskThin, false, BATCH, Pd, Mb, kSrcQueue>()
+               : mixed_fn<kMetricKerr, kDiskNone, false, BATCH, Pd, Mb, kSrcQueue>();
+  return P.disk == kDiskThin
+             ? mixed_fn<kMetricSchwarzschild, kDiskThin, false, BATCH, Pd, Mb, kSrcQueue>()
+             : mixed_fn<kMetricSchwarzschild, kDiskNone, false, BATCH, Pd, Mb, kSrcQueue>();
 }
 
 // Batched launches: the variant (PERIOD, MINB) by index, kBatchVariants of
@@ -422,14 +457,17 @@ const void* select_mixed(const DevParams& P, const BatchTable* batch, int varian
 }  // namespace
 
 cudaError_t mixed_occupancy(const DevParams& P, int* blocks_per_sm, const BatchTable* batch,
-                            int variant) {
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      blocks_per_sm, select_mixed(P, batch, variant), kTraceBlock, 0);
+                            int variant, bool returned) {
+  const void* fn = returned ? (batch ? select_returned<true>(P) : select_returned<false>(P))
+                            : select_mixed(P, batch, variant);
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, fn, kTraceBlock, 0);
 }
 
 cudaError_t launch_mixed(const DevParams& P, const DevOutputs& O, DevControl* ctl, int grid,
-                         cudaStream_t stream, const BatchTable* batch, int variant) {
-  const void* fn = select_mixed(P, batch, variant);
+                         cudaStream_t stream, const BatchTable* batch, int variant,
+                         bool returned) {
+  const void* fn = returned ? (batch ? select_returned<true>(P) : select_returned<false>(P))
+                            : select_mixed(P, batch, variant);
   DevParams p = P;
   DevOutputs o = O;
   BatchTable b{};

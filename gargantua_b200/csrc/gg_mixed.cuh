@@ -317,7 +317,12 @@ GG_DEV int attempt_dp45_mixed(const DevParams& P, MixedRegs& S, const MixedSmem&
     G.at(P, pr, pth);
     float a[4];
     G.accel(pw, a);
-    K.set(s, make_float4(a[0], a[1], a[2], a[3]));
+    // a lane whose k1 is valid keeps it when its warp recomputes stage 0
+    // for a refilled lane: k7 was evaluated at the stage position formed as
+    // an FP32 increment, which differs in the last bits from the
+    // compensated state, so overwriting it would make a ray's result depend
+    // on which rays share its warp
+    if (s > 0 || !k1_valid) K.set(s, make_float4(a[0], a[1], a[2], a[3]));
   }
   float ex[4] = {0.0f, 0.0f, 0.0f, 0.0f}, ev[4] = {0.0f, 0.0f, 0.0f, 0.0f};
   error_sums<0>(K, ex, ev);

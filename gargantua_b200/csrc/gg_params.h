@@ -73,7 +73,9 @@ struct DevParams {
   float mass_f, spin_f, rs_f, atol_f, rtol_f;
   float max_radius_hi, max_radius_lo;  // max_radius as an unevaluated float pair
   float band_r, pole_band;
-  float pad_mixed;
+  // FP64 pass over the band queue: return a ray to the mixed form (the
+  // O.ret queue) once it is clear of the band (gg_trace.cu, kBackMargin)
+  uint32_t hand_back;
   // sampling
   uint32_t width, height, spa, spp, jitter_spp, sub_w, sub_h;
   uint32_t pad0;
@@ -129,10 +131,13 @@ struct DevOutputs {
   double* sample_rgb;   // 3*n linear sample colours, reduced per pixel when spp > 1
   struct QueuedRay* queue;  // mixed form: rays handed to the FP64 pass
   uint64_t queue_cap;
+  struct QueuedRay* ret;    // mixed form: rays the FP64 pass hands back
+  uint64_t ret_cap;
 };
 
-// A ray the mixed-precision pass hands to the FP64 pass: its state at the
-// start of the attempt that entered the FP64 band, in FP64.
+// A ray the mixed-precision pass hands to the FP64 pass (its state at the
+// start of the attempt that entered the FP64 band) or the FP64 pass hands
+// back (its state after the step that left the band), in FP64.
 struct QueuedRay {
   double x[4];
   double v[4];
@@ -193,6 +198,9 @@ struct DevControl {
   unsigned long long queued;     // rays handed to the FP64 pass
   unsigned long long next_queued;  // the FP64 pass's queue head
   unsigned long long fp64_attempts;  // attempts made in the FP64 pass
+  unsigned long long returned;       // rays the FP64 pass handed back to the mixed form
+  unsigned long long next_returned;  // the mixed form's head on that queue
+  unsigned long long band_total;     // hand-offs to the FP64 pass of earlier rounds
 };
 
 }  // namespace gg

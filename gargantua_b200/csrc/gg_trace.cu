@@ -23,9 +23,40 @@ namespace gg {
 
 namespace {
 
+// A ray in the FP64 pass of the mixed form goes back to the FP32 stepper
+// once an accepted step leaves it this far outside the band: r beyond
+// band_r + kBackMargin M and theta more than kBackPole * pole_band from
+// both poles (the margin keeps rays from bouncing between the passes).
+constexpr double kBackMargin = 1.0;
+constexpr double kBackPole = 2.0;
+
+// Writes a ray clear of the band to the return queue (out of line, once per
+// returned ray).
+__device__ __noinline__ void hand_back(const DevOutputs& O, DevControl* ctl, Ray R, uint64_t idx,
+                                       uint32_t n_att, uint32_t n_acc, uint32_t scene) {
+  const unsigned long long slot = atomicAdd(&ctl->returned, 1ull);
+  if (slot >= O.ret_cap) {
+    atomicExch(&ctl->queue_overflow, 1u);
+    return;
+  }
+  QueuedRay& q = O.ret[slot];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    q.x[i] = R.x[i];
+    q.v[i] = R.v[i];
+  }
+  q.h = R.h;
+  q.lam = R.lam;
+  q.idx = idx;
+  q.n_att = n_att;
+  q.n_acc = n_acc;
+  q.scene = scene;
+}
+
 // SRC: kSrcCamera traces the render's samples from the camera; kSrcQueue
 // finishes, in FP64, the rays the mixed-precision pass handed over (their
-// count is read from ctl->queued, which that pass wrote before this launch).
+// count is read from ctl->queued, which that pass wrote before this launch);
+// with P.hand_back it returns rays that leave the band to the mixed form.
 // BATCH (kSrcQueue only): the rays come from a batched render; each carries
 // its scene, whose parameters and outputs are in B.  SCENE (kSrcCamera, no
 // thin disk): every accepted step's chord is tested against P's scene of
@@ -336,6 +367,14 @@ __global__ void __launch_bounds__(kTraceBlock,
         else if (res == kEscaped) done_cls = kClsEscaped;
         else if (n_att >= PL.max_steps) done_cls = kClsMaxSteps;
       }
+      if (SRC == kSrcQueue && P.hand_back && acc && done_cls < 0 &&
+          R.x[1] > (double)PL.band_r + kBackMargin &&
+          fmin(R.x[2], kPi - R.x[2]) > kBackPole * (double)PL.pole_band) {
+        hand_back(O, ctl, R, idx, n_att, n_acc, scene);
+        atomicAdd(&bs.fp64_att, (unsigned long long)(n_att - n_att0));
+        live = false;
+        continue;
+      }
       if (SCENE && done_cls == kClsScene) {
         finish_scene_sample(PL, OL, idx, R, n_att, n_acc, inten, scene_rgb);
         atomicAdd(&bs.attempts, (unsigned long long)n_att);
@@ -489,6 +528,19 @@ cudaError_t launch_trace(const DevParams& P, const DevOutputs& O, DevControl* ct
   BatchTable b{};
   void* args[] = {&p, &o, &ctl, &b};
   return cudaLaunchKernel(fn, dim3(grid), dim3(kTraceBlock), args, 0, stream);
+}
+
+// Between the rounds of the mixed form: the band queue's entries are all
+// consumed; its count moves to the running total and it restarts empty.
+__global__ void next_round_kernel(DevControl* ctl) {
+  ctl->band_total += ctl->queued;
+  ctl->queued = 0;
+  ctl->next_queued = 0;
+}
+
+cudaError_t launch_next_round(DevControl* ctl, cudaStream_t stream) {
+  next_round_kernel<<<1, 1, 0, stream>>>(ctl);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_reduce(const DevParams& P, const double* samples, uint8_t* rgb8, int sms,

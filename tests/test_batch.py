@@ -37,7 +37,29 @@ def _small_batch(n=6):
 
 
 @pytest.mark.gpu
+def test_large_batch_with_hand_back_matches_single_renders(renderer):
+    """A batch above 2^20 samples hands rays that leave the FP64 band back to
+    FP32; those rays then take different (equally accurate) steps than in the
+    single-round renders of the small scenes, so images agree on all but a
+    few pixels."""
+    scenes = workloads.batch_scenes(40, seed=5, max_side=512)
+    assert sum(s.n_samples for s in scenes) >= 1 << 20
+    imgs = renderer.render_batch(scenes)
+    st = renderer.stats()
+    assert st.rays == sum(s.n_samples for s in scenes) and st.fp64_rays > 0
+    same = total = 0
+    for sc, img in zip(scenes, imgs):
+        ref, _ = renderer.render(sc)
+        px = (img == ref).all(axis=2)
+        same += int(px.sum())
+        total += px.size
+    assert same / total > 0.9995, same / total
+
+
+@pytest.mark.gpu
 def test_batch_equals_single_scene_renders(renderer):
+    """Below 2^20 samples a batch and single renders both run one FP64 round,
+    so every ray takes the same steps."""
     scenes = _small_batch()
     imgs = renderer.render_batch(scenes)
     st = renderer.stats()

@@ -96,6 +96,20 @@ def test_mixed_schwarzschild_256_against_oracle(renderer, oracle_mod):
 
 
 @pytest.mark.gpu
+def test_mixed_is_reproducible(renderer):
+    """Each ray's result does not depend on which rays share its warp: two
+    renders of the same frame (dynamic work distribution, so different warp
+    compositions) agree bit for bit."""
+    scene = _mixed(workloads.kerr_thin_1080p)
+    scene.width, scene.height = 640, 360
+    _, a = renderer.render(scene, rays=True)
+    _, b = renderer.render(scene, rays=True)
+    assert np.array_equal(a.cls, b.cls) and np.array_equal(a.attempts, b.attempts)
+    assert np.array_equal(a.x, b.x) and np.array_equal(a.v, b.v)
+    assert np.array_equal(a.rgb, b.rgb)
+
+
+@pytest.mark.gpu
 def test_mixed_unsupported_combinations(renderer):
     ref_stepper = workloads.kerr_thin_1080p(precision=abi.GG_PREC_MIXED)
     with pytest.raises(abi.GargantuaError) as e:
