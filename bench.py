@@ -403,79 +403,105 @@ def run_stress(args) -> None:
     r_ISCO-25 M, 50,000 step() calls per ray: one frame per form (plain FP64,
     FP64 full Dormand-Prince, mixed), timed with CUDA events after a warm-up
     frame of 256 x 256 x 1, and the per-ray attempt distribution.  Per-ray
-    outputs stay on the device (attempts and class only)."""
+    outputs stay on the device (attempts and class only).  With N ranks
+    (torchrun) each traces its interleaved rows of the frame (shard.shard_scene;
+    jitter is keyed by the global sample, so the frame is the same); times
+    are the max over ranks, counts and histograms sums."""
     import torch
 
-    from gargantua_b200 import abi, workloads
+    from gargantua_b200 import abi, shard, workloads
     from gargantua_b200.curved import Renderer
 
     rank, world, local = dist_env()
-    if rank != 0:
-        return
     torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device(f"cuda:{local}"))
     r = Renderer(local)
     side, spp = args.side, args.spp
     n = side * side * spp
-    img = torch.empty(side * side * 3, dtype=torch.uint8, device="cuda")
+    rows = shard.rows_of(side, rank, world)
+    n_mine = rows * side * spp
+    img = torch.empty(max(1, rows) * side * 3, dtype=torch.uint8, device="cuda")
     stream = torch.cuda.ExternalStream(r.stream)
     edges = [0] + [2 ** k for k in range(17)]  # attempts per ray: [0,1), [1,2), [2,4), ...
     forms, cls_of = {}, {}
+
+    def reduce_sum(xs):
+        t = torch.tensor(xs, dtype=torch.int64, device="cuda")
+        if world > 1:
+            import torch.distributed as dist
+            dist.all_reduce(t)
+        return t.tolist()
+
     for form, prec, stepper in (("fp64", abi.GG_PREC_FP64, abi.GG_STEPPER_REFERENCE),
                                 ("fp64_dp45", abi.GG_PREC_FP64, abi.GG_STEPPER_DP45),
                                 ("mixed", abi.GG_PREC_MIXED, abi.GG_STEPPER_DP45)):
         warm = workloads.kerr_stress_4k(precision=prec, side=256, spp=1, stepper=stepper)
         r.render_device(warm, img.data_ptr(), None, r.stream)
-        scene = workloads.kerr_stress_4k(precision=prec, side=side, spp=spp, stepper=stepper)
-        att = torch.empty(n, dtype=torch.int32, device="cuda")
-        cls = torch.empty(n, dtype=torch.int32, device="cuda")
+        scene = shard.shard_scene(
+            workloads.kerr_stress_4k(precision=prec, side=side, spp=spp, stepper=stepper),
+            rank, world)
+        att = torch.empty(n_mine, dtype=torch.int32, device="cuda")
+        cls = torch.empty(n_mine, dtype=torch.int32, device="cuda")
         rays = abi.gg_ray_out_t()
         rays.attempts = C.cast(C.c_void_p(att.data_ptr()), C.POINTER(C.c_uint32))
         rays.cls = C.cast(C.c_void_p(cls.data_ptr()), C.POINTER(C.c_int32))
         stream.synchronize()
+        barrier(world)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         r.render_device(scene, img.data_ptr(), rays, r.stream)
         e1.record(stream)
         stream.synchronize()
-        ms = e0.elapsed_time(e1)
+        ms = max_over_ranks(e0.elapsed_time(e1), world)
         st = r.stats()
         a = att.to(torch.int64)
         hist = [int(((a >= lo) & (a < hi)).sum()) for lo, hi in zip(edges[:-1], edges[1:])]
         hist.append(int((a >= edges[-1]).sum()))
-        q = torch.quantile(a[:: max(1, n // 4_000_000)].double(),
-                           torch.tensor([0.5, 0.9, 0.99, 0.999], dtype=torch.float64,
-                                        device="cuda")).tolist()
-        forms[form] = {"ms": ms, "geodesics_per_s": n / (ms * 1e-3),
-                       "attempts": int(st.attempts), "accepted": int(st.accepted),
-                       "attempts_per_s": st.attempts / (ms * 1e-3),
-                       "class_count": [int(x) for x in st.class_count],
-                       "fp64_band_rays": int(st.fp64_rays),
-                       "fp64_band_attempts": int(st.fp64_attempts),
-                       "attempts_per_ray": {"p50": q[0], "p90": q[1], "p99": q[2], "p99.9": q[3],
-                                            "max": int(a.max())},
-                       "attempts_histogram": {"bin_lower_edges": edges[:-1] + [edges[-1]],
-                                              "counts": hist}}
+        sums = reduce_sum([int(st.attempts), int(st.accepted), int(st.fp64_rays),
+                           int(st.fp64_attempts)] + [int(x) for x in st.class_count] + hist)
+        nc = len(st.class_count)
+        entry = {"ms": ms, "geodesics_per_s": n / (ms * 1e-3),
+                 "attempts": sums[0], "accepted": sums[1],
+                 "attempts_per_s": sums[0] / (ms * 1e-3),
+                 "class_count": sums[4:4 + nc],
+                 "fp64_band_rays": sums[2], "fp64_band_attempts": sums[3],
+                 "attempts_histogram": {"bin_lower_edges": edges[:-1] + [edges[-1]],
+                                        "counts": sums[4 + nc:]}}
+        if world == 1:
+            q = torch.quantile(a[:: max(1, n // 4_000_000)].double(),
+                               torch.tensor([0.5, 0.9, 0.99, 0.999], dtype=torch.float64,
+                                            device="cuda")).tolist()
+            entry["attempts_per_ray"] = {"p50": q[0], "p90": q[1], "p99": q[2], "p99.9": q[3],
+                                         "max": int(a.max())}
+        forms[form] = entry
         cls_of[form] = cls
         del att
-    cpu = None
-    if not args.no_cpu_baseline:
-        cpu = cpu_baseline(workloads.kerr_stress_4k(side=side, spp=spp), 10.0,
-                           f"the {side}x{side}x{spp} spp frame")
+    agree = reduce_sum([int((cls_of["mixed"] == cls_of["fp64_dp45"]).sum())])[0]
     line = {"metric": "Kerr a=0.998 4096^2 x16 spp stress: geodesics/s and per-ray steps",
-            "unit": UNIT, "n_gpus": 1, "higher_is_better": True,
+            "unit": UNIT, "n_gpus": world, "higher_is_better": True, "scaling": "strong",
             "config": {"workload": f"kerr_a0.998_{side}x{side}x{spp}spp_thin_disk",
                        "r_cam": 15.0, "inclination_deg": 85.0, "disk": "r_ISCO-25M",
-                       "max_steps": 50000, "rtol": 1e-8, "atol": 1e-10, "samples": n},
+                       "max_steps": 50000, "rtol": 1e-8, "atol": 1e-10, "samples": n,
+                       "parallelism": f"interleaved rows over {world} rank(s)"},
             "forms": forms,
             "mixed_over_fp64": forms["mixed"]["geodesics_per_s"] / forms["fp64"]["geodesics_per_s"],
             "mixed_over_fp64_dp45": (forms["mixed"]["geodesics_per_s"]
                                      / forms["fp64_dp45"]["geodesics_per_s"]),
-            "class_agreement_mixed_vs_fp64_dp45":
-                float((cls_of["mixed"] == cls_of["fp64_dp45"]).double().mean())}
-    if cpu is not None:
-        line["cpu_baseline"] = cpu
+            "class_agreement_mixed_vs_fp64_dp45": agree / n}
     r.close()
-    print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    if rank == 0:
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(workloads.kerr_stress_4k(side=side, spp=spp), 10.0,
+                                                f"the {side}x{side}x{spp} spp frame")
+        print(json.dumps(line), flush=True)
 
 
 # ---- batched scenes --------------------------------------------------------------------
@@ -484,71 +510,97 @@ def run_batch(args) -> None:
     spin, camera distance and inclination, image side 64..512, disk outer
     radius drawn per scene, seed 0), mixed precision, in one persistent
     launch replayed from a CUDA graph, after autotuning the kernel variant on
-    every 8th scene.  Beside it: the same scenes rendered one launch each."""
+    every 8th scene.  With N ranks (torchrun) each renders the scenes
+    shard.partition_scenes gives it (cost-balanced, no data-path
+    collective); a step is timed as the max over ranks.  Beside it, at N=1:
+    the same scenes rendered one launch each."""
     import torch
 
-    from gargantua_b200 import workloads
+    from gargantua_b200 import shard, workloads
     from gargantua_b200.curved import Renderer
 
     rank, world, local = dist_env()
-    if rank != 0:
-        return
     torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device(f"cuda:{local}"))
     r = Renderer(local)
     scenes = workloads.batch_scenes(args.scenes, seed=0)
+    parts = shard.partition_scenes(scenes, world)
+    mine = [scenes[k] for k in parts[rank]]
     n = sum(sc.n_samples for sc in scenes)
-    pix = sum(sc.width * sc.height for sc in scenes)
+    pix = sum(sc.width * sc.height for sc in mine)
     out = torch.empty(3 * pix, dtype=torch.uint8, device="cuda")
     stream = torch.cuda.ExternalStream(r.stream)
     t0 = time.perf_counter()
-    variant, tune_ms = r.batch_autotune(scenes[::8])
+    variant, tune_ms = r.batch_autotune(mine[::8])
     tune_s = time.perf_counter() - t0
-    steps, warmup = max(1, args.steps // 3), 1
+    steps, warmup = max(1, args.steps // 3), max(3, args.warmup)
     for _ in range(warmup):
-        r.render_batch_device(scenes, out.data_ptr(), r.stream)
+        r.render_batch_device(mine, out.data_ptr(), r.stream)
     stream.synchronize()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-          for _ in range(steps)]
-    for i in range(steps):
-        ev[i][0].record(stream)
-        r.render_batch_device(scenes, out.data_ptr(), r.stream)
-        ev[i][1].record(stream)
-    stream.synchronize()
-    ms = [a.elapsed_time(b) for a, b in ev]
+    ms = []
+    for _ in range(steps):
+        barrier(world)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r.render_batch_device(mine, out.data_ptr(), r.stream)
+        e1.record(stream)
+        stream.synchronize()
+        ms.append(max_over_ranks(e0.elapsed_time(e1), world))
     st = r.stats()
-    # the same scenes, one launch each (single-scene entry point, same kernel family)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    off = 0
-    for sc in scenes[:8]:  # warm the single-scene path
-        r.render_device(sc, out.data_ptr(), None, r.stream)
-    stream.synchronize()
-    e0.record(stream)
-    for sc in scenes:
-        r.render_device(sc, out.data_ptr() + off, None, r.stream)
-        off += 3 * sc.width * sc.height
-    e1.record(stream)
-    stream.synchronize()
-    single_ms = e0.elapsed_time(e1)
+    attempts = sum_over_ranks(int(st.attempts), world)
+    band_rays = sum_over_ranks(int(st.fp64_rays), world)
+    band_att = sum_over_ranks(int(st.fp64_attempts), world)
+    rays = sum_over_ranks(int(st.rays), world)
     best = min(ms)
     line = {"metric": "batched scenes: geodesics/s, 2,048 Kerr scenes of uneven size, mixed",
-            "unit": UNIT, "n_gpus": 1, "higher_is_better": True, "steps": steps,
+            "unit": UNIT, "n_gpus": world, "higher_is_better": True, "steps": steps,
+            "warmup": warmup, "scaling": "strong",
             "config": {"workload": f"batch_{len(scenes)}_kerr_scenes_seed0", "scenes": len(scenes),
                        "samples": n, "sides": "64..512 step 64", "spin": "U[0,0.998]",
                        "r_cam": "U[10,100]", "inclination_deg": "U[5,89]", "r_out": "U[15,40]",
-                       "max_steps": 20000},
+                       "max_steps": 20000,
+                       "parallelism": f"scenes over {world} rank(s), cost-balanced "
+                                      "(shard.partition_scenes)",
+                       "l2": "outputs (3 B per sample, 625 MB) larger than L2"},
             "value": n / (best * 1e-3), "ms_per_batch": ms,
-            "attempts": int(st.attempts), "attempts_per_s": st.attempts / (best * 1e-3),
-            "class_count": [int(x) for x in st.class_count],
-            "fp64_band_rays": int(st.fp64_rays), "fp64_band_attempts": int(st.fp64_attempts),
+            "rays": rays, "attempts": attempts, "attempts_per_s": attempts / (best * 1e-3),
+            "fp64_band_rays": band_rays, "fp64_band_attempts": band_att,
             "autotune": {"variant": variant, "variant_ms_on_every_8th_scene": tune_ms,
                          "variants": "0..5 = (period, CTAs/SM) (16,8) (8,8) (4,8) (16,7) (8,7) (4,7)",
-                         "wall_s": tune_s},
-            "one_launch_per_scene": {"ms": single_ms, "geodesics_per_s": n / (single_ms * 1e-3)},
-            "batch_over_one_launch_per_scene": single_ms / best}
+                         "wall_s": tune_s}}
+    if world == 1:
+        line["class_count"] = [int(x) for x in st.class_count]
+        # the same scenes, one launch each (single-scene entry point, same kernel family)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        off = 0
+        for sc in scenes[:8]:  # warm the single-scene path
+            r.render_device(sc, out.data_ptr(), None, r.stream)
+        stream.synchronize()
+        e0.record(stream)
+        for sc in scenes:
+            r.render_device(sc, out.data_ptr() + off, None, r.stream)
+            off += 3 * sc.width * sc.height
+        e1.record(stream)
+        stream.synchronize()
+        single_ms = e0.elapsed_time(e1)
+        line["one_launch_per_scene"] = {"ms": single_ms,
+                                        "geodesics_per_s": n / (single_ms * 1e-3)}
+        line["batch_over_one_launch_per_scene"] = single_ms / best
+    else:
+        line["samples_per_rank"] = [sum(scenes[k].n_samples for k in p) for p in parts]
     r.close()
-    if not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline_batch(scenes)
-    print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    if rank == 0:
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline_batch(scenes)
+        print(json.dumps(line), flush=True)
 
 
 # ---- reference arm ---------------------------------------------------------------

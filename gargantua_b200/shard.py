@@ -1,5 +1,7 @@
-"""One frame split across GPUs: interleaved image rows per rank and one
-gather of the RGB8 rows to rank 0.
+"""Work split across GPUs.  One frame: interleaved image rows per rank and
+one gather of the RGB8 rows to rank 0.  A batch of scenes: whole scenes per
+rank, balanced by their expected cost (``partition_scenes``); rays never
+cross ranks, so a batch needs no collective on its data path.
 
 Rank k of N traces rows k, k + N, k + 2N, ... (``RenderOptions.row_offset``
 / ``row_step``): the expensive rays -- the shadow's edge and the photon
@@ -38,6 +40,34 @@ def assemble(parts, height: int):
     for k, part in enumerate(parts):
         full[k::world] = part[: rows_of(height, k, world)]
     return full
+
+
+def scene_cost(scene) -> float:
+    """Expected work of a scene: its samples times the expected attempts per
+    ray.  With the step capped at max_step (1 M by default) a ray that
+    escapes needs about (its path in and out) / max_step attempts, roughly
+    (r_cam + max_radius) / max_step; rays near the hole add a bounded
+    share on top."""
+    integ = scene.options.integrator
+    max_radius = integ.max_radius if integ is not None else 200.0
+    max_step = integ.max_step if integ is not None else 1.0
+    r_cam = float(scene.camera.position[1])
+    return float(scene.n_samples) * (r_cam + max_radius) / max(max_step, 1e-12)
+
+
+def partition_scenes(scenes, world: int) -> list:
+    """Scene indices per rank: longest-processing-time-first greedy on
+    scene_cost (each scene to the rank with the least cost so far; ties to
+    the lower rank), each rank's list in ascending index order.
+    Deterministic, so every rank computes the same split."""
+    order = sorted(range(len(scenes)), key=lambda k: (-scene_cost(scenes[k]), k))
+    load = [0.0] * world
+    parts = [[] for _ in range(world)]
+    for k in order:
+        dst = min(range(world), key=lambda j: (load[j], j))
+        parts[dst].append(k)
+        load[dst] += scene_cost(scenes[k])
+    return [sorted(p) for p in parts]
 
 
 def gather_rows(local, height: int, rank: int, world: int, group=None):

@@ -1,7 +1,9 @@
-"""A frame split across GPUs by interleaved rows (gargantua_b200.shard).
+"""Work split across GPUs (gargantua_b200.shard): a frame by interleaved
+rows, a batch by whole scenes.
 
 CPU: the row partition and the assembly, and the gather itself with two
-gloo ranks (127.0.0.1).  GPU: the shards a rank would render, stitched,
+gloo ranks (127.0.0.1); the scene partition's coverage and balance, and that
+two gloo ranks derive the same split.  GPU: the shards a rank would render, stitched,
 equal the unsplit render byte for byte (each ray's arithmetic does not
 depend on which rows share its launch; jitter is keyed by the sample's
 index in the whole image).
@@ -54,6 +56,58 @@ def test_gather_two_gloo_ranks(height):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     procs = [ctx.Process(target=_gather_worker, args=(r, 2, port, height, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+    assert all(p.exitcode == 0 for p in procs)
+    assert all(q.get(timeout=10) for _ in procs)
+
+
+@pytest.mark.parametrize("world", [1, 2, 3, 8])
+def test_scene_partition_covers_and_balances(world):
+    scenes = workloads.batch_scenes(256, seed=0)
+    parts = shard.partition_scenes(scenes, world)
+    assert parts == shard.partition_scenes(scenes, world)  # deterministic
+    flat = sorted(k for p in parts for k in p)
+    assert flat == list(range(len(scenes)))
+    loads = [sum(shard.scene_cost(scenes[k]) for k in p) for p in parts]
+    # longest-processing-time-first: within one scene's cost of the mean
+    biggest = max(shard.scene_cost(s) for s in scenes)
+    assert max(loads) - min(loads) <= biggest
+
+
+def _partition_worker(rank, world, port, q):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        scenes = workloads.batch_scenes(64, seed=1)
+        mine = shard.partition_scenes(scenes, world)[rank]
+        got = [None] * world
+        dist.all_gather_object(got, mine)
+        if rank == 0:
+            flat = sorted(k for p in got for k in p)
+            q.put(flat == list(range(len(scenes))))
+        else:
+            q.put(True)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_scene_partition_two_gloo_ranks():
+    """Every rank derives the same split on its own: together they render
+    every scene exactly once."""
+    import socket
+
+    import torch.multiprocessing as mp
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_partition_worker, args=(r, 2, port, q)) for r in range(2)]
     for p in procs:
         p.start()
     for p in procs:
