@@ -96,6 +96,28 @@ def test_mixed_schwarzschild_256_against_oracle(renderer, oracle_mod):
 
 
 @pytest.mark.gpu
+def test_mixed_schwarzschild_1024_with_hand_back(renderer, oracle_mod):
+    """From 2^20 samples up the FP64 pass hands rays that leave the band back
+    to FP32: the Schwarzschild frame at 1024 x 1024 takes that path and is
+    held to the same criteria (seeded 4,096-ray subset against the oracle;
+    the full frame's classes against the FP64 kernel)."""
+    scene = _mixed(workloads.schwarzschild_thin_256)
+    scene.width = scene.height = 1024
+    _, g = renderer.render(scene, rays=True)
+    st = renderer.stats()
+    assert st.fp64_rays > 0 and st.rays == scene.n_samples
+    ref = workloads.schwarzschild_thin_256(stepper=abi.GG_STEPPER_DP45)
+    ref.width = ref.height = 1024
+    _, g64 = renderer.render(ref, rays=True)
+    assert (g.cls == g64.cls).mean() >= 0.9999
+    idx = np.sort(np.random.default_rng(11).choice(scene.n_samples, 4096, replace=False))
+    oc = oracle_mod.trace_cross(ref, idx.astype(np.uint64))
+    rep = mixed_report(ref, g.cross[:, idx], oc, oracle_mod, index=idx)
+    assert rep["p99"] <= 1e-6, rep
+    assert len(rep["unexplained"]) <= 0.0005 * rep["rays"] + 1, rep
+
+
+@pytest.mark.gpu
 def test_mixed_is_reproducible(renderer):
     """Each ray's result does not depend on which rays share its warp: two
     renders of the same frame (dynamic work distribution, so different warp
