@@ -8,10 +8,13 @@
 // photon orbit, theta within pole_band of a pole, or a step that would carry
 // theta across a pole -- the lane writes the ray's state, in FP64, to a
 // global queue and takes a new sample.  The FP64 kernel then runs over that
-// queue in a second launch (trace_fp64_kernel<..., kSrcQueue>).  Handing rays
-// off instead of running FP64 attempts inside this kernel keeps both launches
-// warp-uniform: a warp never executes the FP32 and the FP64 attempt
-// back to back for lanes in different bands.
+// queue in a second launch (trace_fp64_kernel<..., kSrcQueue>), which, in
+// renders of 2^20 samples or more, hands rays that leave the band back to a
+// return queue; this kernel continues those (SRC = kSrcQueue) in a third
+// launch, and a last FP64 launch finishes the rays that re-entered the band.
+// Handing rays off instead of running FP64 attempts inside this kernel keeps
+// every launch warp-uniform: a warp never executes the FP32 and the FP64
+// attempt back to back for lanes in different bands.
 //
 // Crossings of the escape sphere and the disk plane are detected on the
 // float-pair differences and located in FP64 on the step's continuous
