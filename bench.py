@@ -327,6 +327,8 @@ def run_ours(args) -> None:
     # Dormand-Prince step x attempts, against the FP32 FMA peak (97 % of the
     # attempts run in FP32; the FP64 band's share is reported beside it)
     fpa = flops.attempt_flops("kerr", scene.integrator_c().rtol, abi.GG_STEPPER_DP45)
+    fpa_reduced = flops.reduced_attempt_flops("kerr", scene.integrator_c().rtol,
+                                              abi.GG_STEPPER_DP45)
     fp64_peak = r.fma_peak(fp64=True)
     fp32_peak = r.fma_peak(fp64=False)
     peak = fp32_peak
@@ -374,6 +376,10 @@ def run_ours(args) -> None:
                      "traffic": None,
                      "kernel": "trace_mixed_kernel<Kerr, ThinDisk> + FP64 band pass",
                      "flops_per_attempt": fpa,
+                     # the formulation the kernels run (closed-form sparse Christoffels)
+                     "flops_per_attempt_reduced": fpa_reduced,
+                     "achieved_reduced": achieved * fpa_reduced / fpa / 1e12,
+                     "frac_reduced": achieved * fpa_reduced / fpa / peak,
                      "peak_source": "measured in this run by gg_measure_fma_peak (FMA chains);"
                                     " MEASURED_PEAKS.json has no FP64/FP32 ALU figure"},
         "forms": {k: {kk: vv for kk, vv in v.items()
