@@ -1,9 +1,14 @@
-"""Pins the C++ oracle against the independent pure-Python restatement.
+"""Committed golden vectors.
 
 tests/golden/golden_rays.json is produced by tests/golden/make_golden.py (plain
 Python doubles, written from the Rust source).  Both restatements follow the
 reference's expression order without fused multiply-adds, so they agree to
 the last bit; the test allows 1e-12 relative for libm differences.
+
+tests/golden/oracle_c1_c2.npz is produced by tests/golden/make_oracle_golden.py:
+the oracle's outcomes on the 256 x 256 Schwarzschild and 1080p Kerr parity
+workloads.  The oracle must reproduce it exactly (CPU), and the CUDA path is
+held to it (GPU) without running the oracle.
 """
 from __future__ import annotations
 
@@ -77,3 +82,58 @@ def test_golden_covers_every_class_and_disk_kind():
     assert {0, 1, 2} <= seen
     assert kinds == {"none", "vol", "thin"}
     assert math.isfinite(CASES[0]["rays"][0]["x"][1])
+
+
+# ---- oracle outcomes on the parity workloads (tests/golden/make_oracle_golden.py) ----
+ORACLE_GOLDEN = Path(__file__).resolve().parent / "golden" / "oracle_c1_c2.npz"
+
+
+class _Rays:
+    def __init__(self, x, v, cls):
+        self.x, self.v, self.cls = x, v, cls
+
+
+def _fixture():
+    return np.load(ORACLE_GOLDEN)
+
+
+def test_oracle_reproduces_committed_vectors(oracle_mod):
+    """The oracle still gives the committed outcomes bit for bit: all of C1's
+    classes and attempt counts, and the endpoints of both seeded subsets."""
+    from gargantua_b200 import workloads
+    d = _fixture()
+    c1 = workloads.schwarzschild_thin_256()
+    _, r1 = oracle_mod.render(c1)
+    assert np.array_equal(r1.cls, d["c1_cls"]) and np.array_equal(r1.attempts, d["c1_attempts"])
+    i1 = d["c1_idx"]
+    assert np.array_equal(r1.x[:, i1], d["c1_x"]) and np.array_equal(r1.v[:, i1], d["c1_v"])
+    c2 = workloads.kerr_thin_1080p()
+    r2 = oracle_mod.trace_samples(c2, d["c2_idx"].astype(np.uint64))
+    assert np.array_equal(r2.cls, d["c2_cls"]) and np.array_equal(r2.attempts, d["c2_attempts"])
+    assert np.array_equal(r2.x, d["c2_x"]) and np.array_equal(r2.v, d["c2_v"])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["c1", "c2"])
+def test_gpu_against_committed_vectors(renderer, case):
+    """The CUDA FP64 path against the committed oracle outcomes, with the bar
+    of the oracle parity tests: class on 99.9 % of samples (the rest lie on
+    class boundaries), attempt counts on 99.9 %, endpoints within 1e-9 on
+    99.9 % of the subset."""
+    from gargantua_b200 import workloads
+    from parity import REL, endpoint_err
+    d = _fixture()
+    scene = workloads.schwarzschild_thin_256() if case == "c1" else workloads.kerr_thin_1080p()
+    _, g = renderer.render(scene, rays=True)
+    idx = d[f"{case}_idx"]
+    if case == "c1":
+        assert (g.cls == d["c1_cls"]).mean() >= 0.999
+        assert (g.attempts == d["c1_attempts"]).mean() >= 0.999
+    cls = d[f"{case}_cls"] if case == "c2" else d["c1_cls"][idx]
+    att = d["c2_attempts"] if case == "c2" else d["c1_attempts"][idx]
+    same = g.cls[idx] == cls
+    assert same.mean() >= 0.999
+    assert (g.attempts[idx] == att)[same].mean() >= 0.999
+    o = _Rays(d[f"{case}_x"], d[f"{case}_v"], cls)
+    e = endpoint_err(scene, g.x[:, idx], g.v[:, idx], o)
+    assert (e[same] <= REL).mean() >= 0.999, np.quantile(e[same], 0.999)
