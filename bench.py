@@ -55,6 +55,11 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "Kerr 1080p geodesics/s, mixed-FP32 vs plain FP64 on B200 at stated endpoint error"
 UNIT = "geodesics/s"
+# DRAM bytes (read + write) of one launch of the FP32 pass on the Kerr 1080p
+# frame, measured with ncu (profiles/launches_mixed_kerr_1080p.md): the image
+# and the band queue, and mostly the local-memory records of the once-per-ray
+# out-of-line work (the crossing search's step record, finish, hand-off).
+MIXED_PASS_DRAM_BYTES = 109_360_128 + 966_294_784
 FLUSH_BYTES = 256 << 20
 
 
@@ -373,7 +378,10 @@ def run_ours(args) -> None:
         "gpu_launches": 5 * steps,
         "roofline": {"bound": "fp32", "achieved": achieved / 1e12,
                      "peak": peak / 1e12, "unit": "TFLOP/s", "frac": achieved / peak,
-                     "traffic": None,
+                     # DRAM read + write of the FP32 pass, one launch of this frame
+                     # (ncu dram__bytes_{read,write}.sum; profiles/launches_mixed_kerr_1080p.md)
+                     "traffic": MIXED_PASS_DRAM_BYTES,
+                     "traffic_unit": "bytes per launch of trace_mixed_kernel",
                      "kernel": "trace_mixed_kernel<Kerr, ThinDisk> + FP64 band pass",
                      "flops_per_attempt": fpa,
                      # the formulation the kernels run (closed-form sparse Christoffels)
