@@ -60,6 +60,9 @@ UNIT = "geodesics/s"
 # and the band queue, and mostly the local-memory records of the once-per-ray
 # out-of-line work (the crossing search's step record, finish, hand-off).
 MIXED_PASS_DRAM_BYTES = 109_360_128 + 966_294_784
+# Renders of this many samples or more run the mixed form's hand-back rounds
+# (kHandBackMinRays in gargantua_b200/csrc/gg_capi.cpp).
+HAND_BACK_MIN_SAMPLES = 1 << 20
 FLUSH_BYTES = 256 << 20
 
 
@@ -372,10 +375,10 @@ def run_ours(args) -> None:
         "e2e": {"value": H["full"].n_samples * steps / e2e_s, "unit": UNIT,
                 "h2d_bytes_per_step": abi.load().gg_struct_size(b"launch_params"),
                 "d2h_bytes_per_step": scene.width * scene.rows * 3},
-        # per step: the mixed kernel, the FP64 band pass (which hands rays
-        # clear of the band back), the round reset, the mixed pass over the
-        # returned rays and the last FP64 pass
-        "gpu_launches": 5 * steps,
+        # per step and rank: the mixed kernel and the FP64 band pass; from 2^20
+        # samples per render also the round reset, the mixed pass over the rays
+        # the band pass hands back and the last FP64 pass
+        "gpu_launches": (5 if scene.n_samples >= HAND_BACK_MIN_SAMPLES else 2) * steps,
         "roofline": {"bound": "fp32", "achieved": achieved / 1e12,
                      "peak": peak / 1e12, "unit": "TFLOP/s", "frac": achieved / peak,
                      # DRAM read + write of the FP32 pass, one launch of this frame
