@@ -71,6 +71,24 @@ def dist_env():
             int(os.environ.get("LOCAL_RANK", "0")))
 
 
+def orbit_frame(scene, rank: int, world: int):
+    """`scene` with its camera moved by 2 pi rank / world in azimuth (same r
+    and inclination, still looking at the hole with +z up)."""
+    import copy
+    import math
+    if world <= 1:
+        return scene
+    s = copy.copy(scene)
+    t, r, th, _ = scene.camera.position
+    ph = 2.0 * math.pi * rank / world
+    rhat = (math.sin(th) * math.cos(ph), math.sin(th) * math.sin(ph), math.cos(th))
+    cam = copy.copy(scene.camera)
+    cam.position = (t, r, th, ph)
+    cam.look_at = (-rhat[0], -rhat[1], -rhat[2])
+    s.camera = cam
+    return s
+
+
 def workload_config(scene, form: str) -> dict:
     integ = scene.integrator_c()
     return {"workload": "kerr_a0.9_1920x1080_thin_disk", "form": form,
@@ -166,22 +184,24 @@ def max_over_ranks(x: float, world: int) -> float:
     return float(t.item())
 
 
-def time_form(r, scene, steps, warmup, world, flush, with_clocks, device_index):
-    """Device-timed renders of `scene` (this rank's rows of the frame) with
-    device-resident outputs; with N > 1 ranks each step also gathers every
-    rank's RGB8 rows (NCCL all-gather), the frame's one collective."""
+def time_form(r, scene, steps, warmup, world, flush, with_clocks, device_index, gather_rows):
+    """Device-timed renders of `scene` (this rank's frame, or its rows of the
+    one frame) with device-resident outputs; with `gather_rows` each step also
+    gathers every rank's RGB8 rows (NCCL all-gather), the split frame's one
+    collective."""
     import torch
     rows = scene.rows
     out = torch.empty(scene.width * rows * 3, dtype=torch.uint8, device="cuda")
     gathered = None
-    if world > 1:
+    gather_rows = gather_rows and world > 1
+    if gather_rows:
         import torch.distributed as dist
         max_rows = (scene.height + world - 1) // world
         pad = torch.zeros(max_rows * scene.width * 3, dtype=torch.uint8, device="cuda")
         gathered = torch.empty(world * pad.numel(), dtype=torch.uint8, device="cuda")
 
     def gather():
-        if world > 1:
+        if gather_rows:
             pad[: out.numel()] = out
             dist.all_gather_into_tensor(gathered, pad)
     # everything (flush, events, renders) on the library context's own stream
@@ -195,7 +215,7 @@ def time_form(r, scene, steps, warmup, world, flush, with_clocks, device_index):
     torch.cuda.synchronize()
     clk = ClockSampler(device_index) if with_clocks else None
     with torch.cuda.stream(stream):
-        for _ in range(warmup if world > 1 else 0):
+        for _ in range(warmup if gather_rows else 0):
             gather()
         for i in range(steps):
             flush.zero_()
@@ -308,21 +328,31 @@ def run_ours(args) -> None:
                                 ("fp64_dp45", abi.GG_PREC_FP64, abi.GG_STEPPER_DP45),
                                 ("mixed", abi.GG_PREC_MIXED, abi.GG_STEPPER_DP45)):
         full = workloads.kerr_thin_1080p(precision=prec, stepper=stepper)
-        # N > 1: this rank's interleaved rows of the one frame (strong scaling)
-        scene = shard.shard_scene(full, rank, world) if world > 1 else full
-        res = time_form(r, scene, steps, warmup, world, flush, form == "mixed", local)
+        if world > 1 and args.split == "rows":
+            # this rank's interleaved rows of the one frame (strong scaling)
+            scene = shard.shard_scene(full, rank, world)
+        else:
+            # this rank's own frame: the camera moved by 2 pi rank / N in
+            # azimuth (frames of an orbit; metric and disk are axisymmetric,
+            # so every frame costs the same and only the sky differs)
+            full = scene = orbit_frame(full, rank, world)
+        res = time_form(r, scene, steps, warmup, world, flush, form == "mixed", local,
+                        args.split == "rows")
         st = res["stats"]
         mean_ms = statistics.mean(res["ms"])
         attempts = sum_over_ranks(int(st.attempts), world)
         accepted = sum_over_ranks(int(st.accepted), world)
+        # samples of the whole job per step: one frame split, or a frame per rank
+        job = full.n_samples * (world if args.split == "frames" else 1)
         forms[form] = {
-            "geodesics_per_s": full.n_samples * steps / (res["total_ms"] * 1e-3),
+            "geodesics_per_s": job * steps / (res["total_ms"] * 1e-3),
             "ms_per_step": res["total_ms"] / steps,
             "launch_ms_mean": mean_ms,
             "attempts_per_frame": attempts,
             "accepted_per_frame": accepted,
             "attempts_per_s": attempts * steps / (res["total_ms"] * 1e-3),
             "accepted_steps_per_s": accepted * steps / (res["total_ms"] * 1e-3),
+            "samples_per_step": job,
             "class_count": [int(x) for x in st.class_count],
             "fp64_band_rays": int(st.fp64_rays), "fp64_band_attempts": int(st.fp64_attempts),
             "clocks": res["clocks"], "scene": scene, "full": full, "stats_attempts": st.attempts,
@@ -367,12 +397,14 @@ def run_ours(args) -> None:
     line = {
         "metric": METRIC, "value": H["geodesics_per_s"], "unit": UNIT, "n_gpus": world,
         "steps": steps, "warmup": warmup, "ms_per_step": H["ms_per_step"],
-        "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "higher_is_better": True,
+        "scaling": "strong" if (world > 1 and args.split == "rows") else "weak",
+        "vs_baseline": None,
         "dtype": "f32+f64",
         "data": "synthetic: procedural Kerr scene, seeded checkerboard sky",
         "config": workload_config(scene, head),
         "clocks": H["clocks"],
-        "e2e": {"value": H["full"].n_samples * steps / e2e_s, "unit": UNIT,
+        "e2e": {"value": H["samples_per_step"] * steps / e2e_s, "unit": UNIT,
                 "h2d_bytes_per_step": abi.load().gg_struct_size(b"launch_params"),
                 "d2h_bytes_per_step": scene.width * scene.rows * 3},
         # per step and rank: the mixed kernel and the FP64 band pass; from 2^20
@@ -400,6 +432,10 @@ def run_ours(args) -> None:
         "attempts_per_ray_pct": {"p50": pct[0], "p90": pct[1], "p99": pct[2], "p99.9": pct[3],
                                  "max": pct[4]},
     }
+    line["config"]["parallelism"] = (
+        f"one frame split by interleaved rows over {world} ranks, RGB8 all-gather"
+        if (world > 1 and args.split == "rows") else
+        f"one 1080p frame per rank ({world}), camera orbit in azimuth, no collective")
     line["endpoint_error"] = endpoint
     line["mixed_over_fp64"] = H["geodesics_per_s"] / forms["fp64"]["geodesics_per_s"]
     line["mixed_over_fp64_dp45"] = H["geodesics_per_s"] / forms["fp64_dp45"]["geodesics_per_s"]
@@ -676,6 +712,9 @@ def main() -> None:
                     help="stress: the a=0.998 4096^2 x 16 spp configuration (one frame per "
                          "form); batch: 2,048 scenes of uneven size in one launch")
     ap.add_argument("--scenes", type=int, default=2048, help="batch: number of scenes")
+    ap.add_argument("--split", choices=["frames", "rows"], default="frames",
+                    help="kerr1080p with N > 1: one frame per rank (weak scaling, no "
+                         "collective) or one frame split by rows (strong scaling, an all-gather)")
     ap.add_argument("--side", type=int, default=4096, help="stress: image side")
     ap.add_argument("--spp", type=int, default=16, help="stress: samples per pixel")
     args = ap.parse_args()

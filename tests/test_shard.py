@@ -135,3 +135,22 @@ def test_shards_equal_the_unsplit_render(renderer, form):
         assert img.shape[0] == shard.rows_of(scene.height, k, world)
         parts.append(img)
     assert np.array_equal(shard.assemble(parts, scene.height), full)
+
+
+def test_orbit_frames_cost_the_same(oracle_mod):
+    """bench.py's weak-scaling frames: rank k's camera is rank 0's moved by
+    2 pi k / N in azimuth.  The metric and thin disk are axisymmetric, so every
+    frame has the same classes and attempt counts (only the sky differs)."""
+    import bench
+    base = workloads.kerr_thin_1080p()
+    base.width, base.height = 64, 36
+    frames = [bench.orbit_frame(base, k, 4) for k in range(4)]
+    for f in frames:
+        t, r, th, ph = f.camera.position
+        assert (r, th) == tuple(base.camera.position[1:3])
+        la = np.array(f.camera.look_at)
+        rhat = np.array([np.sin(th) * np.cos(ph), np.sin(th) * np.sin(ph), np.cos(th)])
+        assert np.allclose(la, -rhat, atol=1e-15)
+    outs = [oracle_mod.render(f)[1] for f in frames[:2]]
+    assert np.array_equal(outs[0].cls, outs[1].cls)
+    assert np.array_equal(outs[0].attempts, outs[1].attempts)
