@@ -56,10 +56,10 @@ sys.path.insert(0, str(ROOT))
 METRIC = "Kerr 1080p geodesics/s, mixed-FP32 vs plain FP64 on B200 at stated endpoint error"
 UNIT = "geodesics/s"
 # DRAM bytes (read + write) of one launch of the FP32 pass on the Kerr 1080p
-# frame, measured with ncu (profiles/launches_mixed_kerr_1080p.md): the image
-# and the band queue, and mostly the local-memory records of the once-per-ray
-# out-of-line work (the crossing search's step record, finish, hand-off).
-MIXED_PASS_DRAM_BYTES = 109_360_128 + 966_294_784
+# frame, measured with ncu (profiles/launches_mixed_kerr_1080p.md): the 6.2 MB
+# image, the band queue and the argument records of the once-per-ray finish
+# and hand-off calls.
+MIXED_PASS_DRAM_BYTES = 4_125_440 + 30_498_048
 # Renders of this many samples or more run the mixed form's hand-back rounds
 # (kHandBackMinRays in gargantua_b200/csrc/gg_capi.cpp).
 HAND_BACK_MIN_SAMPLES = 1 << 20

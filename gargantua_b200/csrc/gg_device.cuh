@@ -812,6 +812,61 @@ static __device__ __noinline__ double dense_crossing(const StepSpan& sp, int com
   return s;
 }
 
+// The same, for a step whose data a source object reads where it lives
+// (Src::xb(c), vb(c), xa(c), va(c), k(l, c), h), one component at a time:
+// no step record is built.  COMP is the component whose crossing is sought;
+// the same arithmetic as dense_comp / dense_crossing, so the same results.
+template <class Src>
+GG_DEV DenseComp dense_comp_src(const Src& sp, int c) {
+  DenseComp q;
+  double w = 0.0;
+  if (c < 4) {
+#pragma unroll
+    for (int l = 0; l < 6; ++l) w = fma(kDP.Dbar[l], sp.k(l, c), w);
+    q.y0 = sp.xb(c);
+    q.r2 = sp.xa(c) - sp.xb(c);
+    q.r3 = sp.h * sp.vb(c) - q.r2;
+    q.r4 = q.r2 - sp.h * sp.va(c) - q.r3;
+    q.r5 = sp.h * sp.h * w;
+  } else {
+    const int i = c - 4;
+#pragma unroll
+    for (int l = 0; l < 7; ++l) w = fma(kDP.D[l], sp.k(l, i), w);
+    q.y0 = sp.vb(i);
+    q.r2 = sp.va(i) - sp.vb(i);
+    q.r3 = sp.h * sp.k(0, i) - q.r2;
+    q.r4 = q.r2 - sp.h * sp.k(6, i) - q.r3;
+    q.r5 = sp.h * w;
+  }
+  return q;
+}
+
+template <int COMP, class Src>
+GG_DEV double dense_crossing_src(const Src& sp, double target, double out[8]) {
+  const DenseComp q = dense_comp_src(sp, COMP);
+  const double flo = q.at(0.0) - target;
+  const double fhi = q.at(1.0) - target;
+  double lo = 0.0, hi = 1.0;
+  double s = flo / (flo - fhi);
+  if (!(s >= 0.0 && s <= 1.0)) s = 0.5;
+  for (int it = 0; it < 30; ++it) {
+    const double fs = q.at(s) - target;
+    if (fs == 0.0) break;
+    if ((fs < 0.0) == (flo < 0.0)) lo = s; else hi = s;
+    const double d = q.slope(s);
+    double sn = d != 0.0 ? s - fs / d : 0.5 * (lo + hi);
+    if (!(sn > lo && sn < hi)) sn = 0.5 * (lo + hi);
+    if (fabs(sn - s) <= 1e-15) {
+      s = sn;
+      break;
+    }
+    s = sn;
+  }
+#pragma unroll
+  for (int c = 0; c < 8; ++c) out[c] = dense_comp_src(sp, c).at(s);
+  return s;
+}
+
 // ---------------------------------------------------------------------------
 // Camera rays (crates/raytracer/src/curved/{camera,ray}.rs) with the
 // reference's rounding: the camera frame is prepared on the host; here only

@@ -81,6 +81,21 @@ __device__ __noinline__ void mixed_finish(const DevParams& P, const DevOutputs& 
   atomicAdd(&bs->cls[cls], 1ull);
 }
 
+// An accepted step's data for its continuous extension, read where it lives:
+// the pre-step state in FP64 (B), the increments and the seven stage
+// derivatives in this lane's shared-memory column (no step record in local
+// memory).
+struct MixedSpan {
+  MixedSmem K;
+  Ray B;
+  double h;
+  GG_DEV double xb(int c) const { return B.x[c]; }
+  GG_DEV double vb(int c) const { return B.v[c]; }
+  GG_DEV double xa(int c) const { return B.x[c] + (double)K.comp(kSlotDx, c); }
+  GG_DEV double va(int c) const { return B.v[c] + (double)K.comp(kSlotDv, c); }
+  GG_DEV double k(int l, int c) const { return (double)K.comp(l, c); }
+};
+
 // The accepted step (pre-step state, increments in slots 7, 8, k1 in slot
 // 0, k7 in slot 6) crossed the escape sphere (`esc`) and/or the disk
 // plane (`dsk`): locate the crossings in FP64 on the step's continuous
@@ -96,29 +111,12 @@ __device__ __noinline__ uint32_t mixed_crossings(const DevParams& P, const DevOu
                                              uint32_t n_att, uint32_t n_acc, BlockStats* bs) {
   const Ray B = mixed_fp64(K, S);
   const uint64_t idx = K.idx();
-  const float4 dx4 = K.get(kSlotDx), dv4 = K.get(kSlotDv);
-  const float dx[4] = {dx4.x, dx4.y, dx4.z, dx4.w}, dv[4] = {dv4.x, dv4.y, dv4.z, dv4.w};
-  StepSpan sp;
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    sp.xb[i] = B.x[i];
-    sp.vb[i] = B.v[i];
-    sp.xa[i] = B.x[i] + (double)dx[i];
-    sp.va[i] = B.v[i] + (double)dv[i];
-  }
-  for (int l = 0; l < 7; ++l) {
-    const float4 k = K.get(l);
-    sp.k[l][0] = k.x;
-    sp.k[l][1] = k.y;
-    sp.k[l][2] = k.z;
-    sp.k[l][3] = k.w;
-  }
-  sp.h = (double)hf;
+  const MixedSpan sp{K, B, (double)hf};
   bool esc_end = false;
   double sky_th = 0.0, sky_ph = 0.0;
   if (esc && (O.cross || P.sky == kSkyChecker)) {
     double c[8];
-    dense_crossing(sp, 1, P.max_radius, c);
+    dense_crossing_src<1>(sp, P.max_radius, c);
     normalize_coords(c);
     if (O.cross) store_cross(P, O, idx, c);
     esc_end = P.sky == kSkyChecker;
@@ -127,7 +125,7 @@ __device__ __noinline__ uint32_t mixed_crossings(const DevParams& P, const DevOu
   }
   if (DISK == kDiskThin && dsk) {
     double c[8];
-    const double s = dense_crossing(sp, 2, kHalfPi, c);
+    const double s = dense_crossing_src<2>(sp, kHalfPi, c);
     normalize_coords(c);
     const double r_c = c[1];
     if (r_c >= P.r_inner && r_c <= P.r_outer) {
@@ -156,8 +154,8 @@ __device__ __noinline__ uint32_t mixed_crossings(const DevParams& P, const DevOu
     Ray end;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-      end.x[i] = sp.xa[i];
-      end.v[i] = sp.va[i];
+      end.x[i] = sp.xa(i);
+      end.v[i] = sp.va(i);
     }
     normalize_coords(end.x);
     end.h = S.h;
