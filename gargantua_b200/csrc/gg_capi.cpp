@@ -286,6 +286,16 @@ void build_params(const gg_metric_t* metric, const gg_camera_t* camera, const gg
   P.rs_f = (float)P.rs;
   P.atol_f = std::fmax((float)P.atol, 1.17549435e-38f);  // keep the scale of a 0 component > 0
   P.rtol_f = (float)P.rtol;
+  {
+    const double m = P.mass, a = P.spin;
+    P.a2_f = (float)(a * a);
+    P.m2_f = (float)(2.0 * m);
+    P.mm2a2_f = (float)(-2.0 * a * a);
+    P.m2a_f = (float)(2.0 * m * a);
+    P.m4a_f = (float)(4.0 * m * a);
+    P.m2a2_f = (float)(2.0 * m * a * a);
+    P.m4a2_f = (float)(4.0 * m * a * a);
+  }
   P.max_radius_hi = (float)P.max_radius;
   P.max_radius_lo = (float)(P.max_radius - (double)P.max_radius_hi);
   // FP64 band: within 0.5 M of the prograde photon orbit or of the horizon

@@ -76,6 +76,9 @@ struct DevParams {
   // FP64 pass over the band queue: return a ray to the mixed form (the
   // O.ret queue) once it is clear of the band (gg_trace.cu, kBackMargin)
   uint32_t hand_back;
+  // the FP32 Kerr right-hand side's per-render constants: a^2, 2M, -2a^2,
+  // 2Ma, 4Ma, 2Ma^2, 4Ma^2
+  float a2_f, m2_f, mm2a2_f, m2a_f, m4a_f, m2a2_f, m4a2_f;
   // sampling
   uint32_t width, height, spa, spp, jitter_spp, sub_w, sub_h;
   uint32_t pad0;
