@@ -211,3 +211,39 @@ def test_dp45_kerr_1080p_seeded_subset(renderer, oracle_mod):
     d[3] = np.abs(np.remainder(gc[3, m] - oc[3, m] + np.pi, 2 * np.pi) - np.pi)
     rel = d.max(axis=0) / np.abs(oc[:, m]).max(axis=0)
     assert np.quantile(rel, 0.999) < 1e-9, np.quantile(rel, 0.999)
+
+
+@pytest.mark.parametrize("w,h", [(1, 1), (1, 37), (33, 1), (7, 5), (31, 3)])
+def test_tiny_and_ragged_frames(renderer, oracle_mod, w, h):
+    """Frames smaller than one 32-sample chunk or not a multiple of it: every
+    sample traced once, classes and endpoints as the oracle's (FP64), classes
+    as the FP64 kernel's (mixed form)."""
+    scene = workloads.kerr_thin_1080p()
+    scene.width, scene.height = w, h
+    img, g = renderer.render(scene, rays=True)
+    st = renderer.stats()
+    assert st.rays == w * h and sum(st.class_count) == w * h and img.shape == (h, w, 3)
+    oimg, o = oracle_mod.render(scene)
+    assert np.array_equal(g.cls, o.cls) and np.array_equal(g.attempts, o.attempts)
+    assert np.array_equal(img, oimg)
+    mixed = workloads.kerr_thin_1080p(precision=abi.GG_PREC_MIXED, stepper=abi.GG_STEPPER_DP45)
+    ref = workloads.kerr_thin_1080p(stepper=abi.GG_STEPPER_DP45)
+    for s in (mixed, ref):
+        s.width, s.height = w, h
+    imgm, gm = renderer.render(mixed, rays=True)
+    assert renderer.stats().rays == w * h
+    _, g64 = renderer.render(ref, rays=True)
+    assert np.array_equal(gm.cls, g64.cls)
+
+
+def test_batch_with_tiny_scenes(renderer):
+    """A batch whose scenes include 1 x 1 and odd-sized frames: each image as
+    the single-scene render's."""
+    scenes = workloads.batch_scenes(5, seed=9, max_side=128)
+    for s, (w, h) in zip(scenes, [(1, 1), (3, 2), (64, 64), (5, 33), (17, 1)]):
+        s.width, s.height = w, h
+    imgs = renderer.render_batch(scenes)
+    assert renderer.stats().rays == sum(s.n_samples for s in scenes)
+    for s, img in zip(scenes, imgs):
+        ref, _ = renderer.render(s)
+        assert img.shape == (s.height, s.width, 3) and np.array_equal(img, ref)
