@@ -1056,7 +1056,11 @@ GG_API int gg_set_hdri(gg_ctx* c, const float* rgb, uint32_t width, uint32_t hei
   int st = grow(&buf, &c->hdri_cap, bytes);
   c->hdri = static_cast<float*>(buf);
   if (st != GG_OK) return st;
-  if (cudaMemcpy(c->hdri, rgb, bytes, cudaMemcpyHostToDevice) != cudaSuccess) return GG_ERR_CUDA;
+  // on the context's (non-blocking) stream and waited for: a copy from
+  // pageable memory may otherwise return before it has landed
+  if (cudaMemcpyAsync(c->hdri, rgb, bytes, cudaMemcpyHostToDevice, c->stream) != cudaSuccess ||
+      cudaStreamSynchronize(c->stream) != cudaSuccess)
+    return GG_ERR_CUDA;
   c->hdri_w = width;
   c->hdri_h = height;
   c->hdri_intensity = intensity;
@@ -1082,8 +1086,11 @@ GG_API int gg_set_scene(gg_ctx* c, const gg_prim_t* prims, uint32_t n) {
   if (st != GG_OK) return st;
   st = grow(&c->scene_nodes, &c->scene_nodes_cap, nb);
   if (st != GG_OK) return st;
-  if (cudaMemcpy(c->scene_prims, ps.data(), pb, cudaMemcpyHostToDevice) != cudaSuccess ||
-      cudaMemcpy(c->scene_nodes, nodes.data(), nb, cudaMemcpyHostToDevice) != cudaSuccess)
+  if (cudaMemcpyAsync(c->scene_prims, ps.data(), pb, cudaMemcpyHostToDevice, c->stream) !=
+          cudaSuccess ||
+      cudaMemcpyAsync(c->scene_nodes, nodes.data(), nb, cudaMemcpyHostToDevice, c->stream) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(c->stream) != cudaSuccess)
     return GG_ERR_CUDA;
   c->scene_set = true;
   return GG_OK;
