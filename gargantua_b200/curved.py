@@ -19,6 +19,7 @@ FP32/FP64 precision form, and per-sample outcome arrays.
 from __future__ import annotations
 
 import ctypes as C
+import itertools
 import math
 from dataclasses import dataclass, field
 from typing import Optional, Union
@@ -113,6 +114,11 @@ class CheckerSky:
     seed: int = 0
 
 
+# Serial numbers of sky maps and scenes, by which a Renderer knows what it
+# has uploaded.
+_SERIALS = itertools.count(1)
+
+
 class HdriSky:
     """Equirectangular environment map (sky.rs:43-123): linear RGB float32
     texels, shape (height, width, 3), row 0 at the +z pole, columns wrapping
@@ -149,6 +155,8 @@ class HdriSky:
             raise ValueError("HdriSky pixels must be (height, width, 3)")
         self.pixels = px
         self.version = getattr(self, "version", 0) + 1
+        if not hasattr(self, "_serial"):
+            self._serial = next(_SERIALS)
 
     @property
     def width(self) -> int:
@@ -159,7 +167,8 @@ class HdriSky:
         return self.pixels.shape[0]
 
     def key(self):
-        return (id(self), self.version, self.intensity)
+        # a serial number, not id(): a new object may reuse a freed one's id
+        return (self._serial, self.version, self.intensity)
 
 
 @dataclass
@@ -230,6 +239,7 @@ class SceneObjects:
     def __init__(self, objects=()):
         self.objects = []
         self.version = 0
+        self._serial = next(_SERIALS)
         for o in objects:
             self.add(o)
 
@@ -244,7 +254,7 @@ class SceneObjects:
         return len(self.objects)
 
     def key(self):
-        return (id(self), self.version)
+        return (self._serial, self.version)
 
     def to_c(self):
         arr = (abi.gg_prim_t * len(self.objects))()
