@@ -33,6 +33,11 @@ inclination, image side 64..512 and disk drawn per scene) in one persistent
 launch from a CUDA graph, with the autotuned kernel variant, against the same
 scenes rendered one launch each.
 
+``--workload adjoint`` times the differentiable render's gradient: Kerr
+512 x 512, L2 image loss, forward with checkpoints and the adjoint to five
+parameters (spin, inclination, r_cam, disk r_in, emissivity index), against
+the central differences it replaces, on the GPU and through the oracle.
+
 ``--impl reference`` times the CPU restatement of the reference's renderer
 (the oracle; the Rust reference cannot be built here) on the host cores on
 a bounded seeded sample of the same frame.
@@ -656,6 +661,211 @@ def run_batch(args) -> None:
         print(json.dumps(line), flush=True)
 
 
+# ---- differentiable render ----------------------------------------------------------
+def cpu_baseline_fd(dscene, p, target_s: float = 20.0) -> dict:
+    """The central differences the adjoint replaces (ten forwards, h = 1e-6
+    relative per parameter) through the oracle on the host cores: each of the
+    ten parameter points traced on the same seeded rays of the image, sized
+    for about `target_s` seconds in all, extrapolated to the whole image;
+    gradients/s."""
+    import numpy as np
+    from oracle import oracle
+    rng = np.random.default_rng(0)
+    threads = len(os.sched_getaffinity(0))
+    n_img = dscene.width * dscene.height
+    points = []
+    for i in range(5):
+        h = 1e-6 * abs(p[i])
+        for sgn in (1.0, -1.0):
+            q = np.array(p, dtype=np.float64)
+            q[i] += sgn * h
+            points.append(dscene.scene_at(q))
+    probe = np.sort(rng.choice(n_img, 512, replace=False)).astype(np.uint64)
+    t0 = time.perf_counter()
+    oracle.trace_samples(points[0], probe, threads=threads)
+    per_ray = (time.perf_counter() - t0) / 512
+    n = int(min(n_img, max(1024, target_s / 10.0 / per_ray)))
+    idx = np.sort(rng.choice(n_img, n, replace=False)).astype(np.uint64)
+    el = 0.0
+    for sc in points:
+        t0 = time.perf_counter()
+        oracle.trace_samples(sc, idx, threads=threads)
+        el += time.perf_counter() - t0
+    fd_s = el * n_img / n
+    return {"value": 1.0 / fd_s, "unit": "gradients/s", "cores": threads, "kind": "port",
+            "seconds_per_gradient": fd_s,
+            "sample": f"{n} seeded rays of the {dscene.width}x{dscene.height} image (rng seed 0) "
+                      f"at each of the 10 central-difference points, {el:.1f} s on {threads} "
+                      "host threads, extrapolated to the whole image"}
+
+
+def run_adjoint(args) -> None:
+    """The differentiation configuration: Kerr 512 x 512, L2 loss of the image
+    against a target rendered at (a = 0.7, inclination 60 deg, r_cam = 40 M,
+    r_in = r_ISCO, q = 3), parameters perturbed by N(0, 5 %) (seed 0).  A step
+    is one gradient: the forward with checkpoints every 32 accepted steps
+    (gg_forward_ckpt), dL/d(image), and the adjoint (gg_backward) to the five
+    parameters.  With N ranks (torchrun) each differentiates its interleaved
+    rows and the five sums are all-reduced (NCCL) inside the step, the one
+    collective; the step time is the max over ranks.  Beside it at N=1: the
+    central differences the adjoint replaces (ten forwards at p +- 1e-6 p_i) on
+    the GPU, and through the oracle on the host cores (cpu_baseline)."""
+    import numpy as np
+    import torch
+
+    from gargantua_b200 import abi, diff, flops
+    from gargantua_b200.curved import Renderer
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device(f"cuda:{local}"))
+    r = Renderer(local)
+    whole = diff.DiffScene()
+    dscene = whole.shard(rank, world)
+    dr = diff.DiffRenderer(dscene, r)
+    stream = torch.cuda.ExternalStream(r.stream)
+    p = diff.perturbed_params(0)
+    target = torch.empty(dr.n_values, dtype=torch.float64, device="cuda")
+    img = torch.empty_like(target)
+    dl = torch.empty_like(target)
+    flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    dr.forward_into(diff.target_params(), target.data_ptr(), r.stream)
+    stream.synchronize()
+
+    def gradient(ev=None):
+        with torch.cuda.stream(stream):
+            if ev:
+                ev[0].record(stream)
+            dr.forward_into(p, img.data_ptr(), r.stream)
+            if ev:
+                ev[1].record(stream)
+            torch.sub(img, target, out=dl)
+            dl.mul_(2.0)
+            if ev:
+                ev[2].record(stream)
+            g = dr.backward(dl.data_ptr(), r.stream)
+            g = diff.allreduce_grad(g)
+            if ev:
+                ev[3].record(stream)
+        return g
+
+    steps, warmup = args.steps, max(3, args.warmup)
+    for _ in range(warmup):
+        g = gradient()
+    stream.synchronize()
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(steps)]
+    barrier(world)
+    torch.cuda.synchronize()
+    clk = ClockSampler(local)
+    for i in range(steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        g = gradient(ev[i])
+    stream.synchronize()
+    clocks = clk.stop()
+    fwd = [e[0].elapsed_time(e[1]) for e in ev]
+    bwd = [e[2].elapsed_time(e[3]) for e in ev]
+    step_ms = [e[0].elapsed_time(e[3]) for e in ev]
+    total_ms = max_over_ranks(sum(step_ms), world)
+    fwd_ms = max_over_ranks(statistics.mean(fwd), world)
+    bwd_ms = max_over_ranks(statistics.mean(bwd), world)
+    ms = total_ms / steps
+    n_img = whole.width * whole.height
+
+    # end to end through the torch.autograd.Function (parameters from the
+    # host, loss and dL/dp back to the host every step)
+    tgt = target.view(dscene.rows, dscene.width, 3)
+    e2e_loss = 0.0
+
+    def e2e_step():
+        pt = torch.tensor(p, dtype=torch.float64, requires_grad=True)
+        out = diff.kerr_image(pt, dr)
+        loss = ((out - tgt) ** 2).sum()
+        loss.backward()
+        gg = diff.allreduce_grad(pt.grad.numpy())
+        return float(loss.item()), gg
+    for _ in range(warmup):
+        e2e_step()
+    torch.cuda.synchronize()
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        e2e_loss, g_e2e = e2e_step()
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    barrier(world)
+
+    # the forward's FP64 attempts (those of the plain render of the same
+    # image), against the FP64 FMA peak
+    r.render(dscene.scene_at(p))
+    attempts = sum_over_ranks(int(r.stats().attempts), world)
+    fpa = flops.attempt_flops("kerr", whole.integrator.rtol, abi.GG_STEPPER_DP45)
+    fp64_peak = r.fma_peak(fp64=True)
+    achieved = attempts / world * fpa / (fwd_ms * 1e-3)
+
+    line = {"metric": "Kerr 512^2 adjoint: gradients/s (forward + backward, 5 parameters)",
+            "value": steps / (total_ms * 1e-3), "unit": "gradients/s", "n_gpus": world,
+            "steps": steps, "warmup": warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: procedural Kerr scene, seeded checkerboard sky",
+            "config": {"workload": "kerr_adjoint_512x512_5_params",
+                       "target": {"spin": 0.7, "inclination_deg": 60.0, "r_cam": 40.0,
+                                  "r_in": "r_ISCO", "emissivity_index": 3.0},
+                       "perturbation": "x (1 + N(0, 0.05)), numpy seed 0",
+                       "params": list(diff.PARAMS), "loss": "L2 over the linear RGB image",
+                       "checkpoint_every_accepted_steps": 32,
+                       "max_steps": whole.max_steps, "rtol": whole.integrator.rtol,
+                       "atol": whole.integrator.atol,
+                       "parallelism": (f"interleaved rows over {world} ranks, all-reduce of the "
+                                       "5 gradient sums" if world > 1 else "one GPU"),
+                       "l2": "256 MiB write between timed steps"},
+            "clocks": clocks,
+            "geodesics_per_s": n_img / (ms * 1e-3),
+            "forward_ms": fwd_ms, "backward_ms": bwd_ms,
+            "gradient": [float(x) for x in g],
+            "e2e": {"value": steps / e2e_s, "unit": "gradients/s",
+                    "h2d_bytes_per_step": abi.load().gg_struct_size(b"launch_params"),
+                    "d2h_bytes_per_step": 5 * 8 + 8,
+                    "via": "diff.kerr_image (torch.autograd.Function) + loss.backward()"},
+            "gpu_launches": 2 * steps,
+            "roofline": {"bound": "fp64", "achieved": achieved / 1e12, "peak": fp64_peak / 1e12,
+                         "unit": "TFLOP/s", "frac": achieved / fp64_peak, "traffic": None,
+                         "kernel": "diff_forward_kernel (the backward's dual-number work is "
+                                   "not counted)",
+                         "flops_per_attempt": fpa, "forward_attempts": attempts,
+                         "peak_source": "measured in this run by gg_measure_fma_peak (FMA chains)"}}
+    if world == 1:
+        # central differences on the GPU: ten forwards and their losses
+        fd = torch.empty_like(target)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            for i in range(5):
+                h = 1e-6 * abs(p[i])
+                for sgn in (1.0, -1.0):
+                    q = np.array(p)
+                    q[i] += sgn * h
+                    dr.forward_into(q, fd.data_ptr(), r.stream)
+                    ((fd - target) ** 2).sum()
+            e1.record(stream)
+        stream.synchronize()
+        fd_ms = e0.elapsed_time(e1)
+        line["central_differences_gpu"] = {"ms": fd_ms, "adjoint_speedup": fd_ms / ms}
+        line["e2e"]["loss"] = e2e_loss
+    r.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    if rank == 0:
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline_fd(whole, p)
+        print(json.dumps(line), flush=True)
+
+
 # ---- reference arm ---------------------------------------------------------------
 def run_reference(args) -> None:
     import numpy as np
@@ -708,9 +918,11 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["kerr1080p", "stress", "batch"], default="kerr1080p",
+    ap.add_argument("--workload", choices=["kerr1080p", "stress", "batch", "adjoint"],
+                    default="kerr1080p",
                     help="stress: the a=0.998 4096^2 x 16 spp configuration (one frame per "
-                         "form); batch: 2,048 scenes of uneven size in one launch")
+                         "form); batch: 2,048 scenes of uneven size in one launch; adjoint: "
+                         "the 512^2 five-parameter gradient")
     ap.add_argument("--scenes", type=int, default=2048, help="batch: number of scenes")
     ap.add_argument("--split", choices=["frames", "rows"], default="frames",
                     help="kerr1080p with N > 1: one frame per rank (weak scaling, no "
@@ -724,6 +936,8 @@ def main() -> None:
         run_stress(args)
     elif args.workload == "batch":
         run_batch(args)
+    elif args.workload == "adjoint":
+        run_adjoint(args)
     else:
         run_ours(args)
 

@@ -1126,7 +1126,7 @@ GG_API int gg_forward_ckpt(gg_ctx* c, const gg_metric_t* metric, double r_cam,
   if (metric->kind != GG_METRIC_KERR || disk->kind != GG_DISK_THIN ||
       integ->precision != GG_PREC_FP64 || integ->stepper != GG_STEPPER_DP45 ||
       opts->samples_per_axis > 1 || opts->jitter_spp > 0 || opts->attempt_budget != 0 ||
-      opts->row_step > 1 || opts->sky == GG_SKY_HDRI || opts->scene)
+      opts->sky == GG_SKY_HDRI || opts->scene)
     return GG_ERR_UNSUPPORTED;
   Lock lock(c);
   DevParams P;

@@ -319,8 +319,11 @@ GG_API int gg_batch_set_variant(gg_ctx* ctx, int variant);
  * budget.  Writes the linear RGB image (width*height*3 doubles, row-major,
  * device pointer) on `stream` and keeps, in the context, per-ray
  * checkpoints of the state every 32 accepted steps for gg_backward.
- * The image is a function of p = (spin, inclination, r_cam, disk r_inner,
- * disk emissivity_index). */
+ * With opts->row_step > 1 only the rows row_offset, row_offset + row_step,
+ * ... are traced and the image holds those rows, in order (one rank's share
+ * of a data-parallel gradient: the ranks' gg_backward results add up to the
+ * whole image's).  The image is a function of p = (spin, inclination, r_cam,
+ * disk r_inner, disk emissivity_index). */
 GG_API int gg_forward_ckpt(gg_ctx* ctx, const gg_metric_t* metric, double r_cam,
                            double inclination, double fov_y_radians, double aspect,
                            const gg_disk_t* disk, const gg_integrator_t* integ,

@@ -7,6 +7,11 @@ respect to the five parameters must match central finite differences of the
 f64 forward (h = 1e-6 relative) to 1e-4 relative.  Pixels whose colour jumps
 between the +h and -h renders (a class or sky-cell boundary crossed: the
 image is piecewise smooth) are left out of that loss for both.
+
+Data parallel: rank k of N differentiates rows k, k + N, ... of the image;
+the forward's rows equal those of the whole image bit for bit, and the
+ranks' gradients (one all-reduce of five numbers; two gloo ranks on the CPU)
+add up to the whole image's.
 """
 from __future__ import annotations
 
@@ -14,6 +19,8 @@ import math
 
 import numpy as np
 import pytest
+
+import os
 
 from gargantua_b200 import abi, diff
 from gargantua_b200.curved import Camera, CheckerSky, RenderOptions, Scene, ThinDisk
@@ -27,6 +34,83 @@ def test_target_and_perturbation_are_seeded():
     a, b = diff.perturbed_params(0), diff.perturbed_params(0)
     assert np.array_equal(a, b) and not np.array_equal(a, t)
     assert np.all(np.abs(a / t - 1.0) < 0.25)
+
+
+@pytest.mark.parametrize("height,world", [(512, 1), (512, 4), (95, 3), (5, 8)])
+def test_row_shards_partition_the_image(height, world):
+    s = diff.DiffScene(width=16, height=height)
+    shards = [s.shard(k, world) for k in range(world)]
+    assert sum(x.rows for x in shards) == height
+    rows = sorted(r for x in shards for r in range(x.row_offset, height, x.row_step))
+    assert rows == list(range(height))
+    assert all(x.width == s.width and x.max_steps == s.max_steps for x in shards)
+
+
+def _allreduce_worker(rank, world, port, q):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        part = np.arange(5, dtype=np.float64) * (rank + 1) + 0.25
+        q.put((rank, diff.allreduce_grad(part).tolist()))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gradient_allreduce_two_gloo_ranks():
+    """Each rank's dL/dp over its rows, summed over the group."""
+    import socket
+
+    import torch.multiprocessing as mp
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_allreduce_worker, args=(r, 2, port, q)) for r in range(2)]
+    for pr in procs:
+        pr.start()
+    for pr in procs:
+        pr.join(120)
+    assert all(pr.exitcode == 0 for pr in procs)
+    want = (np.arange(5, dtype=np.float64) * 3 + 0.5).tolist()
+    got = dict(q.get(timeout=10) for _ in procs)
+    assert got[0] == want and got[1] == want
+
+
+def test_gradient_allreduce_single_process_is_identity():
+    g = np.array([1.5, -2.0, 0.0, 3.25, 1e-9])
+    assert np.array_equal(diff.allreduce_grad(g), g)
+
+
+@pytest.mark.gpu
+def test_row_shards_add_up_to_the_whole_gradient(renderer):
+    """Rank k of 3 on rows k::3 (95 rows: 32, 32, 31), one after another on
+    one context: each shard's image is those rows of the whole image, and
+    the shards' gradients sum to the whole image's."""
+    import torch
+    s = diff.DiffScene(width=96, height=95)
+    full = diff.DiffRenderer(s, renderer)
+    target = full.render(diff.target_params()).clone()
+    p = diff.perturbed_params()
+    img = full.render(p).clone()
+    dl = (2.0 * (img - target)).contiguous()
+    torch.cuda.current_stream().synchronize()
+    g_full = full.backward(dl.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    world = 3
+    g_sum = np.zeros(5)
+    for k in range(world):
+        dr = diff.DiffRenderer(s.shard(k, world), renderer)
+        img_k = dr.render(p)
+        assert img_k.shape == (len(range(k, s.height, world)), s.width, 3)
+        assert torch.equal(img_k, img[k::world])
+        dl_k = dl[k::world].contiguous()
+        torch.cuda.current_stream().synchronize()
+        g_sum += dr.backward(dl_k.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    assert np.all(g_full != 0.0)
+    # the same per-pixel terms, summed in another order (block partials, atomics)
+    assert np.allclose(g_sum, g_full, rtol=1e-9, atol=0.0), (g_sum, g_full)
 
 
 @pytest.mark.gpu
