@@ -9,9 +9,10 @@
 // horizon pixels are piecewise constant in the parameters (zero gradient;
 // their jumps across class or cell boundaries are not differentiated).
 //
-// Forward (diff_forward_kernel): one ray per thread, the same FP64 attempt
-// as the FP64 kernel with its stage derivatives in local memory; the state
-// (x, v, next h) is checkpointed every kCkptEvery accepted steps.
+// Forward (gg_forward_ckpt): the FP64 trace kernel's checkpointing variant
+// (trace_fp64_kernel<Kerr, thin disk, full Dormand-Prince, ..., CKPT> in
+// gg_trace.cu), which also stores each ray's state (x, v, next h) at the start
+// and after every kCkptEvery-th accepted step, and its DiffRay.
 //
 // Backward (diff_backward_kernel), per disk ray, given dL/d(colour):
 //   1. the crossing step (the last accepted step) again in forward-mode dual
@@ -46,8 +47,6 @@ namespace gg {
 
 namespace {
 
-constexpr int kCkptEvery = 32;
-
 // a^mu of one Kerr right-hand side in dual arithmetic (no r clamp: valid
 // stages have r > 0).
 template <int N>
@@ -75,107 +74,6 @@ GG_DEV T redshift_eq(double M, const T& a, const T& r, const T v[4]) {
   const T p_phi = gtph * v[0] + gphph * v[3];
   const T e_emit = -(p_t * u_t + p_phi * u_p);
   return -p_t / e_emit;
-}
-
-// Finish colour of a disk crossing (same as the FP64 kernel).
-GG_DEV void disk_rgb(const DevParams& P, double r_c, const double c[8], double rgb[3]) {
-  const double g = redshift_factor<kMetricKerr>(P, r_c, kHalfPi, c + 4);
-  const double q = P.r_inner / r_c;
-  const double g2 = g * g;
-  disk_color((g2 * g2) * ::pow(q, P.emissivity_index), rgb);
-}
-
-__global__ void __launch_bounds__(128) diff_forward_kernel(const __grid_constant__ DevParams P,
-                                                           const __grid_constant__ DiffOut D) {
-  for (uint64_t idx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < P.n_rays;
-       idx += (uint64_t)gridDim.x * blockDim.x) {
-    double kl[7][4];
-    const KStoreLocal K{kl};
-    Ray R = start_sample(P, idx);
-    Ckpt* ck = D.ckpt + idx * D.ckpt_per_ray;
-    uint32_t n_ckpt = 0, n_acc = 0, n_att = 0;
-    auto save = [&]() {
-      if (n_ckpt < D.ckpt_per_ray) {
-        Ckpt& k = ck[n_ckpt];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          k.x[i] = R.x[i];
-          k.v[i] = R.v[i];
-        }
-        k.h = R.h;
-      }
-      ++n_ckpt;
-    };
-    save();
-    bool k1v = false, k7p = false;
-    int cls = kClsMaxSteps;
-    double rgb[3] = {0.0, 0.0, 10.0 / 255.0};
-    while (n_att < P.max_steps) {
-      double xb[4], vb[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        xb[i] = R.x[i];
-        vb[i] = R.v[i];
-      }
-      bool acc;
-      double h_used = 0.0;
-      StepEnd end;
-      const int res = attempt_dp45_fp64<kMetricKerr>(P, R, K, k1v, k7p, acc, h_used, end);
-      n_att += 1;
-      if (res == kHorizon) {
-        cls = kClsHorizon;
-        rgb[0] = rgb[1] = rgb[2] = 0.0;
-        break;
-      }
-      if (res == kEscaped) {
-        cls = kClsEscaped;
-        checker_sky(P, R.x[2], R.x[3], rgb);
-        break;
-      }
-      if (!acc) continue;
-      n_acc += 1;
-      const bool esc = xb[1] <= P.max_radius && end.xraw[1] > P.max_radius;
-      const double d_b = xb[2] - kHalfPi, d_a = R.x[2] - kHalfPi;
-      const bool dsk = (d_b < 0.0 && d_a >= 0.0) || (d_b > 0.0 && d_a <= 0.0);
-      if (esc || dsk) {
-        StepSpan sp;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          sp.xb[i] = xb[i];
-          sp.vb[i] = vb[i];
-          sp.xa[i] = end.xraw[i];
-          sp.va[i] = R.v[i];
-        }
-        for (int l = 0; l < 7; ++l)
-#pragma unroll
-          for (int i = 0; i < 4; ++i) sp.k[l][i] = kl[l][i];
-        sp.h = h_used;
-        if (dsk) {
-          double c[8];
-          dense_crossing(sp, 2, kHalfPi, c);
-          normalize_coords(c);
-          if (c[1] >= P.r_inner && c[1] <= P.r_outer) {
-            cls = kClsDisk;
-            c[2] = kHalfPi;
-            disk_rgb(P, c[1], c, rgb);
-            break;
-          }
-        }
-        if (esc && P.sky == kSkyChecker) {  // the cell at the escape crossing
-          double c[8];
-          dense_crossing(sp, 1, P.max_radius, c);
-          normalize_coords(c);
-          cls = kClsEscaped;
-          checker_sky(P, c[2], c[3], rgb);
-          break;
-        }
-      }
-      if (n_acc % kCkptEvery == 0) save();
-    }
-    D.rays[idx] = DiffRay{n_acc, n_ckpt, cls, 0u};
-#pragma unroll
-    for (int c = 0; c < 3; ++c) D.rgb[3 * idx + c] = rgb[c];
-  }
 }
 
 // ---- backward -----------------------------------------------------------------
@@ -526,15 +424,6 @@ __global__ void __launch_bounds__(128) diff_backward_kernel(const __grid_constan
 }
 
 }  // namespace
-
-cudaError_t launch_diff_forward(const DevParams& P, const DiffOut& D, int sms,
-                                cudaStream_t stream) {
-  const uint64_t blocks_needed = (P.n_rays + 127) / 128;
-  uint64_t grid = (uint64_t)sms * 8;
-  if (grid > blocks_needed) grid = blocks_needed;
-  diff_forward_kernel<<<(unsigned)(grid < 1 ? 1 : grid), 128, 0, stream>>>(P, D);
-  return cudaGetLastError();
-}
 
 cudaError_t launch_diff_backward(const DevParams& P, const DiffOut& D, const double* dl_drgb,
                                  double* grad5, int sms, cudaStream_t stream) {

@@ -1131,19 +1131,22 @@ GG_API int gg_forward_ckpt(gg_ctx* c, const gg_metric_t* metric, double r_cam,
   Lock lock(c);
   DevParams P;
   build_params(metric, &cam, disk, integ, opts, width, height, &P);
-  const uint32_t cpr = integ->max_steps / 32 + 2;
+  P.ckpt = 1;
+  const uint32_t cpr = integ->max_steps / gg::kCkptEvery + 2;
   int st = grow(&c->diff_rays, &c->diff_rays_cap, sizeof(gg::DiffRay) * P.n_rays);
   if (st != GG_OK) return st;
   st = grow(&c->diff_ckpt, &c->diff_ckpt_cap, sizeof(gg::Ckpt) * cpr * P.n_rays);
   if (st != GG_OK) return st;
-  gg::DiffOut D{static_cast<gg::DiffRay*>(c->diff_rays), static_cast<gg::Ckpt*>(c->diff_ckpt),
-                cpr, 0u, rgb_lin_dev};
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
-  if (cudaStreamWaitEvent(s, c->ev_done, 0) != cudaSuccess) return GG_ERR_CUDA;
-  if (cudaEventRecord(c->ev_start, s) != cudaSuccess) return GG_ERR_CUDA;
-  if (gg::launch_diff_forward(P, D, c->sms, s) != cudaSuccess) return GG_ERR_CUDA;
-  if (cudaEventRecord(c->ev_stop, s) != cudaSuccess) return GG_ERR_CUDA;
-  if (cudaEventRecord(c->ev_done, s) != cudaSuccess) return GG_ERR_CUDA;
+  // the FP64 trace kernel's checkpointing variant: linear colour per ray,
+  // checkpoints and DiffRay
+  DevOutputs O{};
+  O.rgb = rgb_lin_dev;
+  O.ckpt = static_cast<gg::Ckpt*>(c->diff_ckpt);
+  O.diff_rays = static_cast<gg::DiffRay*>(c->diff_rays);
+  O.ckpt_per_ray = cpr;
+  c->diff_ready = false;
+  st = enqueue(c, P, O, false, static_cast<cudaStream_t>(stream));
+  if (st != GG_OK) return st;
   c->diff_P = P;
   c->diff_ckpt_per_ray = cpr;
   c->diff_ready = true;
@@ -1166,7 +1169,7 @@ GG_API int gg_backward(gg_ctx* c, const double* dl_drgb_dev, double grad[5], voi
     return GG_ERR_OOM;
   }
   gg::DiffOut D{static_cast<gg::DiffRay*>(c->diff_rays), static_cast<gg::Ckpt*>(c->diff_ckpt),
-                c->diff_ckpt_per_ray, 0u, nullptr};
+                c->diff_ckpt_per_ray, 0u};
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (cudaStreamWaitEvent(s, c->ev_done, 0) != cudaSuccess) return GG_ERR_CUDA;
   if (cudaMemsetAsync(c->diff_grad, 0, 5 * sizeof(double), s) != cudaSuccess) return GG_ERR_CUDA;

@@ -57,11 +57,9 @@ cudaError_t launch_queue_trace(const DevParams& P, const DevOutputs& O, DevContr
                                int grid, cudaStream_t stream,
                                const BatchTable* batch = nullptr);
 
-// Differentiable render: the forward pass with checkpoints and the adjoint
-// pass (gg_adjoint.cu); grad5 (device) accumulates dL/d(a, inclination,
-// r_cam, r_inner, q).
-cudaError_t launch_diff_forward(const DevParams& P, const DiffOut& D, int sms,
-                                cudaStream_t stream);
+// Differentiable render: the adjoint pass (gg_adjoint.cu) of a forward run
+// by launch_trace with P.ckpt set; grad5 (device) accumulates dL/d(a,
+// inclination, r_cam, r_inner, q).
 cudaError_t launch_diff_backward(const DevParams& P, const DiffOut& D, const double* dl_drgb,
                                  double* grad5, int sms, cudaStream_t stream);
 

@@ -112,7 +112,9 @@ struct DevParams {
   const ScenePrim* prims;
   const SceneNode* nodes;
   uint32_t scene;
-  uint32_t pad_scene;
+  // gg_forward_ckpt: the FP64 kernel also stores each ray's checkpoints and
+  // DiffRay (DevOutputs::ckpt, diff_rays)
+  uint32_t ckpt;
   // control
   uint64_t attempt_budget;
   double inv_spp;
@@ -136,6 +138,10 @@ struct DevOutputs {
   uint64_t queue_cap;
   struct QueuedRay* ret;    // mixed form: rays the FP64 pass hands back
   uint64_t ret_cap;
+  struct Ckpt* ckpt;         // differentiable render: ckpt_per_ray entries per ray
+  struct DiffRay* diff_rays;
+  uint32_t ckpt_per_ray;
+  uint32_t pad_ckpt;
 };
 
 // A ray the mixed-precision pass hands to the FP64 pass (its state at the
@@ -167,17 +173,18 @@ struct DiffRay {
   int32_t cls;
   uint32_t pad;
 };
+// Accepted steps between checkpoints of the differentiable render's forward.
+constexpr int kCkptEvery = 32;
 struct Ckpt {  // state after every kCkptEvery-th accepted step, and the next step size
   double x[4];
   double v[4];
   double h;
 };
-struct DiffOut {
+struct DiffOut {  // what the backward pass reads
   DiffRay* rays;
   Ckpt* ckpt;          // ckpt_per_ray entries per ray
   uint32_t ckpt_per_ray;
   uint32_t pad;
-  double* rgb;         // 3 per ray: linear colour (the differentiated image)
 };
 
 // Where a batched launch finds its scenes: first[k] is the global index of

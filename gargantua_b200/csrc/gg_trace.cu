@@ -60,8 +60,11 @@ __device__ __noinline__ void hand_back(const DevOutputs& O, DevControl* ctl, Ray
 // BATCH (kSrcQueue only): the rays come from a batched render; each carries
 // its scene, whose parameters and outputs are in B.  SCENE (kSrcCamera, no
 // thin disk): every accepted step's chord is tested against P's scene of
-// objects first.
-template <int METRIC, int DISK, int STEPPER, int SRC, bool BATCH, bool SCENE>
+// objects first.  CKPT (kSrcCamera, Kerr, thin disk, full Dormand-Prince):
+// the differentiable render's forward, which also stores each ray's state
+// (x, v, next h) at its start and after every kCkptEvery-th accepted step it
+// survives (O.ckpt) and, when it ends, its DiffRay (O.diff_rays).
+template <int METRIC, int DISK, int STEPPER, int SRC, bool BATCH, bool SCENE, bool CKPT>
 __global__ void __launch_bounds__(kTraceBlock,
                                   METRIC == kMetricKerr ? kTraceMinBlocksKerr : kTraceMinBlocksSchw)
     trace_fp64_kernel(const __grid_constant__ DevParams P, const __grid_constant__ DevOutputs O,
@@ -95,6 +98,19 @@ __global__ void __launch_bounds__(kTraceBlock,
   bool crossed = false;
   bool k1_valid = false;    // K(0, .) holds a(x, v) of the current state
   bool k7_pending = false;  // full DP: K(6, .) is the next k1, copy pending
+  uint32_t n_ckpt = 0;      // CKPT: checkpoints of the ray so far
+  auto save_ckpt = [&]() {
+    if (n_ckpt < O.ckpt_per_ray) {
+      Ckpt& c = O.ckpt[idx * O.ckpt_per_ray + n_ckpt];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        c.x[i] = R.x[i];
+        c.v[i] = R.v[i];
+      }
+      c.h = R.h;
+    }
+    ++n_ckpt;
+  };
 
   uint64_t wbase = 0;
   uint32_t wcount = 0;
@@ -153,6 +169,10 @@ __global__ void __launch_bounds__(kTraceBlock,
           R = start_sample(P, idx);
           n_att = 0;
           n_acc = 0;
+          if (CKPT) {
+            n_ckpt = 0;
+            save_ckpt();
+          }
         }
         live = true;
         inten = 0.0;
@@ -367,6 +387,11 @@ __global__ void __launch_bounds__(kTraceBlock,
         else if (res == kEscaped) done_cls = kClsEscaped;
         else if (n_att >= PL.max_steps) done_cls = kClsMaxSteps;
       }
+      // a checkpoint after every kCkptEvery-th accepted step that did not end
+      // the ray at a crossing (a step that runs out of attempts still counts)
+      if (CKPT && acc && (done_cls < 0 || done_cls == kClsMaxSteps) &&
+          n_acc % kCkptEvery == 0)
+        save_ckpt();
       if (SRC == kSrcQueue && P.hand_back && acc && done_cls < 0 &&
           R.x[1] > (double)PL.band_r + kBackMargin &&
           fmin(R.x[2], kPi - R.x[2]) > kBackPole * (double)PL.pole_band) {
@@ -385,6 +410,7 @@ __global__ void __launch_bounds__(kTraceBlock,
       } else if (done_cls >= 0) {
         finish(PL, OL, idx, done_cls, R, n_att, n_acc, out_int, out_temp, crossed,
                sky_at_cross ? sky_th : R.x[2], sky_at_cross ? sky_ph : R.x[3]);
+        if (CKPT) O.diff_rays[idx] = DiffRay{n_acc, n_ckpt, done_cls, 0u};
         if (SRC == kSrcQueue) atomicAdd(&bs.fp64_att, (unsigned long long)(n_att - n_att0));
         budget_pending += n_att;
         live = false;
@@ -442,10 +468,11 @@ __global__ void reduce_samples_kernel(const __grid_constant__ DevParams P, const
   }
 }
 
-template <int METRIC, int DISK, int STEPPER, int SRC, bool BATCH = false, bool SCENE = false>
+template <int METRIC, int DISK, int STEPPER, int SRC, bool BATCH = false, bool SCENE = false,
+          bool CKPT = false>
 const void* trace_fn() {
   return reinterpret_cast<const void*>(
-      &trace_fp64_kernel<METRIC, DISK, STEPPER, SRC, BATCH, SCENE>);
+      &trace_fp64_kernel<METRIC, DISK, STEPPER, SRC, BATCH, SCENE, CKPT>);
 }
 
 // With a scene: no disk or the volumetric one (the reference's
@@ -477,6 +504,9 @@ const void* select_metric_disk(const DevParams& P) {
 }
 
 const void* select_trace(const DevParams& P) {
+  // gg_forward_ckpt admits only Kerr, the thin disk and the full stepper
+  if (P.ckpt)
+    return trace_fn<kMetricKerr, kDiskThin, kStepperDP45, kSrcCamera, false, false, true>();
   return P.stepper == kStepperDP45 ? select_metric_disk<kStepperDP45>(P)
                                    : select_metric_disk<kStepperReference>(P);
 }
