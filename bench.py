@@ -834,8 +834,8 @@ def run_adjoint(args) -> None:
             "gpu_launches": 2 * steps,
             "roofline": {"bound": "fp64", "achieved": achieved / 1e12, "peak": fp64_peak / 1e12,
                          "unit": "TFLOP/s", "frac": achieved / fp64_peak, "traffic": None,
-                         "kernel": "diff_forward_kernel (the backward's dual-number work is "
-                                   "not counted)",
+                         "kernel": "trace_fp64_kernel<Kerr, ThinDisk, DP45, camera, CKPT> (the "
+                                   "forward; the backward's dual-number work is not counted)",
                          "flops_per_attempt": fpa, "forward_attempts": attempts,
                          "peak_source": "measured in this run by gg_measure_fma_peak (FMA chains)"}}
     if world == 1:

@@ -66,6 +66,8 @@ struct gg_ctx {
   size_t diff_rays_cap = 0;
   void* diff_ckpt = nullptr;
   size_t diff_ckpt_cap = 0;
+  void* diff_list = nullptr;  // the backward pass's sorted work list
+  size_t diff_list_cap = 0;
   double* diff_grad = nullptr;       // 5 doubles, device
   double* diff_grad_host = nullptr;  // pinned
   // equirectangular sky map (gg_set_hdri), RGB float texels on the device
@@ -902,6 +904,7 @@ GG_API int gg_destroy(gg_ctx* c) {
   if (c->batch_host) cudaFreeHost(c->batch_host);
   if (c->diff_rays) cudaFree(c->diff_rays);
   if (c->diff_ckpt) cudaFree(c->diff_ckpt);
+  if (c->diff_list) cudaFree(c->diff_list);
   if (c->diff_grad) cudaFree(c->diff_grad);
   if (c->diff_grad_host) cudaFreeHost(c->diff_grad_host);
   if (c->hdri) cudaFree(c->hdri);
@@ -1168,13 +1171,16 @@ GG_API int gg_backward(gg_ctx* c, const double* dl_drgb_dev, double grad[5], voi
     c->diff_grad_host = nullptr;
     return GG_ERR_OOM;
   }
+  const int gl = grow(&c->diff_list, &c->diff_list_cap,
+                     gg::backward_list_bytes(c->diff_P.n_rays, c->diff_ckpt_per_ray));
+  if (gl != GG_OK) return gl;
   gg::DiffOut D{static_cast<gg::DiffRay*>(c->diff_rays), static_cast<gg::Ckpt*>(c->diff_ckpt),
                 c->diff_ckpt_per_ray, 0u};
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (cudaStreamWaitEvent(s, c->ev_done, 0) != cudaSuccess) return GG_ERR_CUDA;
   if (cudaMemsetAsync(c->diff_grad, 0, 5 * sizeof(double), s) != cudaSuccess) return GG_ERR_CUDA;
-  if (gg::launch_diff_backward(c->diff_P, D, dl_drgb_dev, c->diff_grad, c->sms, s) !=
-      cudaSuccess)
+  if (gg::launch_diff_backward(c->diff_P, D, dl_drgb_dev, c->diff_grad, c->diff_list, c->sms,
+                               s) != cudaSuccess)
     return GG_ERR_CUDA;
   if (cudaMemcpyAsync(c->diff_grad_host, c->diff_grad, 5 * sizeof(double),
                       cudaMemcpyDeviceToHost, s) != cudaSuccess)

@@ -60,8 +60,10 @@ cudaError_t launch_queue_trace(const DevParams& P, const DevOutputs& O, DevContr
 // Differentiable render: the adjoint pass (gg_adjoint.cu) of a forward run
 // by launch_trace with P.ckpt set; grad5 (device) accumulates dL/d(a,
 // inclination, r_cam, r_inner, q).
+// list_buf (device, backward_list_bytes) holds the pass's sorted work list.
+size_t backward_list_bytes(uint64_t n_rays, uint32_t n_keys);
 cudaError_t launch_diff_backward(const DevParams& P, const DiffOut& D, const double* dl_drgb,
-                                 double* grad5, int sms, cudaStream_t stream);
+                                 double* grad5, void* list_buf, int sms, cudaStream_t stream);
 
 // Best-of-5 FMA throughput (FLOP/s, FMA = 2) of the current device.
 cudaError_t measure_fma_peak(int fp64, int sms, double* flops);
