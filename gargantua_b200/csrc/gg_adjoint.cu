@@ -439,13 +439,21 @@ GG_DEV bool backward_key(const DiffOut& D, const double* dl, uint64_t idx, uint3
   return true;
 }
 
+// Neighbouring disk rays mostly share a key: the lanes of a warp with the
+// same key take their slots with one atomic (count and scatter), which keeps
+// the popular bins from serialising.  The loops run the same trips on every
+// lane of a block, so the warp-wide votes see all 32 lanes.
 __global__ void backward_count_kernel(const __grid_constant__ DevParams P,
                                       const __grid_constant__ DiffOut D, const double* dl,
                                       BackwardList L) {
-  for (uint64_t idx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < P.n_rays;
-       idx += (uint64_t)gridDim.x * blockDim.x) {
-    uint32_t k;
-    if (backward_key(D, dl, idx, &k)) atomicAdd(L.bins + k, 1u);
+  const unsigned lane = threadIdx.x & 31u;
+  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < P.n_rays;
+       base += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t idx = base + threadIdx.x;
+    uint32_t k = 0;
+    const bool has = idx < P.n_rays && backward_key(D, dl, idx, &k);
+    const unsigned grp = __match_any_sync(kFull, has ? k : 0xffffffffu);
+    if (has && lane == (unsigned)(__ffs(grp) - 1)) atomicAdd(L.bins + k, (uint32_t)__popc(grp));
   }
 }
 
@@ -479,10 +487,20 @@ __global__ void __launch_bounds__(kScanThreads) backward_scan_kernel(BackwardLis
 __global__ void backward_scatter_kernel(const __grid_constant__ DevParams P,
                                         const __grid_constant__ DiffOut D, const double* dl,
                                         BackwardList L) {
-  for (uint64_t idx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < P.n_rays;
-       idx += (uint64_t)gridDim.x * blockDim.x) {
-    uint32_t k;
-    if (backward_key(D, dl, idx, &k)) L.list[atomicAdd(L.bins + k, 1u)] = idx;
+  const unsigned lane = threadIdx.x & 31u;
+  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < P.n_rays;
+       base += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t idx = base + threadIdx.x;
+    uint32_t k = 0;
+    const bool has = idx < P.n_rays && backward_key(D, dl, idx, &k);
+    const unsigned grp = __match_any_sync(kFull, has ? k : 0xffffffffu);
+    if (has) {
+      const unsigned leader = (unsigned)(__ffs(grp) - 1);
+      uint32_t first = 0;
+      if (lane == leader) first = atomicAdd(L.bins + k, (uint32_t)__popc(grp));
+      first = __shfl_sync(grp, first, leader);
+      L.list[first + (uint32_t)__popc(grp & lanemask_lt())] = idx;
+    }
   }
 }
 

@@ -1,10 +1,13 @@
 """Render one named workload a few times, for profilers and quick timings.
 
     python -m gargantua_b200.profile_run --workload kerr_thin_1080p --precision mixed
+    python -m gargantua_b200.profile_run --workload adjoint_512 --repeats 3
 
 Prints the device time and statistics of each render.  Under a profiler,
 select the trace launch with its kernel name (trace_mixed_kernel,
-trace_fp64_kernel).
+trace_fp64_kernel).  adjoint_512 renders the differentiable render's target
+once, then runs `repeats` gradients (forward with checkpoints, dL/d(image),
+backward) of the 512 x 512 five-parameter configuration.
 """
 from __future__ import annotations
 
@@ -18,7 +21,32 @@ WORKLOADS = {
     "kerr_thin_1080p": workloads.kerr_thin_1080p,
     "schwarzschild_thin_256": workloads.schwarzschild_thin_256,
     "kerr_stress_4k": workloads.kerr_stress_4k,
+    "adjoint_512": None,
 }
+
+
+def run_adjoint(repeats: int) -> None:
+    import torch
+
+    from . import diff
+    r = Renderer(0)
+    dr = diff.DiffRenderer(diff.DiffScene(), r)
+    target = dr.render(diff.target_params()).clone()
+    p = diff.perturbed_params(0)
+    stream = torch.cuda.current_stream()
+    for _ in range(repeats):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        img = dr.render(p)
+        st = r.stats()
+        dl = (2.0 * (img - target)).contiguous()
+        g = dr.backward(dl.data_ptr(), stream.cuda_stream)
+        e1.record(stream)
+        stream.synchronize()
+        print(json.dumps({"workload": "adjoint_512", "gradient_ms": e0.elapsed_time(e1),
+                          "forward_attempts": st.attempts, "gradient": [float(x) for x in g]}),
+              flush=True)
+    r.close()
 
 
 def main() -> None:
@@ -31,6 +59,9 @@ def main() -> None:
     ap.add_argument("--side", type=int, default=None, help="kerr_stress_4k: image side")
     ap.add_argument("--spp", type=int, default=None, help="kerr_stress_4k: samples per pixel")
     a = ap.parse_args()
+    if a.workload == "adjoint_512":
+        run_adjoint(a.repeats)
+        return
     prec = abi.GG_PREC_MIXED if a.precision == "mixed" else abi.GG_PREC_FP64
     stepper = a.stepper or ("dp45" if a.precision == "mixed" else "reference")
     kw = {"precision": prec,
