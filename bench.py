@@ -38,6 +38,10 @@ scenes rendered one launch each.
 parameters (spin, inclination, r_cam, disk r_in, emissivity index), against
 the central differences it replaces, on the GPU and through the oracle.
 
+``--workload features`` times the paths beside it on the reference CLI's
+800 x 600 render: the volumetric disk, a sky map, the lensed-spheres scene,
+and the command line end to end to a PNG file, each against the oracle.
+
 ``--impl reference`` times the CPU restatement of the reference's renderer
 (the oracle; the Rust reference cannot be built here) on the host cores on
 a bounded seeded sample of the same frame.
@@ -866,6 +870,126 @@ def run_adjoint(args) -> None:
         print(json.dumps(line), flush=True)
 
 
+# ---- the next-tier paths ---------------------------------------------------------------
+def feature_scenes():
+    """The reference CLI's render (800 x 600, camera r = 30 M on the equator,
+    procedural sky, FP64 reference step; crates/gr-renderer/src/main.rs:78-137)
+    with each path beside the thin-disk ray path: the volumetric disk, a sky
+    map, and the lensed-spheres scene."""
+    from gargantua_b200 import workloads
+    from gargantua_b200.curved import HdriSky
+    cases = {}
+    cases["volumetric_disk_schwarzschild"] = workloads.reference_cli(disk=True)
+    cases["volumetric_disk_kerr_a0.9"] = workloads.reference_cli(metric="kerr", disk=True)
+    sc = workloads.reference_cli(metric="kerr")
+    sc.options.sky = HdriSky(workloads.synthetic_sky_map())
+    cases["sky_map_kerr_a0.9"] = sc
+    sc = workloads.reference_cli()
+    sc.objects = workloads.lensed_spheres()
+    cases["lensed_spheres_schwarzschild"] = sc
+    sc = workloads.reference_cli(metric="kerr", disk=True)
+    sc.objects = workloads.lensed_spheres()
+    cases["lensed_spheres_volumetric_disk_kerr_a0.9"] = sc
+    return cases
+
+
+def run_features(args) -> None:
+    """The paths beside the thin-disk ray path, each timed on the GPU (CUDA
+    events, device output) and through the oracle on the host cores (a seeded
+    sample of the same render): the reference's volumetric disk, its sky map,
+    its scene chords (lensed spheres), and the command line end to end to a
+    PNG file (wall clock).  One GPU; under torchrun the other ranks exit."""
+    import numpy as np
+    import torch
+
+    from gargantua_b200 import cli
+    from gargantua_b200.curved import Renderer
+    from oracle import oracle
+
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    r = Renderer(local)
+    stream = torch.cuda.ExternalStream(r.stream)
+    flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    threads = len(os.sched_getaffinity(0))
+    steps, warmup = args.steps, max(3, args.warmup)
+    rng = np.random.default_rng(0)
+    cases, clk_all = {}, []
+    for name, sc in feature_scenes().items():
+        img = torch.empty(sc.width * sc.height * 3, dtype=torch.uint8, device="cuda")
+        for _ in range(warmup):
+            r.render_device(sc, img.data_ptr(), None, r.stream)
+        stream.synchronize()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(steps)]
+        clk = ClockSampler(local)
+        with torch.cuda.stream(stream):
+            for e0, e1 in ev:
+                flush.zero_()
+                e0.record(stream)
+                r.render_device(sc, img.data_ptr(), None, r.stream)
+                e1.record(stream)
+        stream.synchronize()
+        clk_all.append(clk.stop())
+        ms = [a.elapsed_time(b) for a, b in ev]
+        st = r.stats()
+        n = sc.n_samples
+        # the oracle on a seeded sample sized for about 3 s
+        probe = np.sort(rng.choice(n, 256, replace=False)).astype(np.uint64)
+        t0 = time.perf_counter()
+        oracle.trace_samples(sc, probe, threads=threads)
+        per = (time.perf_counter() - t0) / 256
+        m = int(min(n, max(1024, 3.0 / max(per, 1e-9))))
+        idx = np.sort(rng.choice(n, m, replace=False)).astype(np.uint64)
+        t0 = time.perf_counter()
+        oracle.trace_samples(sc, idx, threads=threads)
+        el = time.perf_counter() - t0
+        best = statistics.median(ms)
+        cases[name] = {"width": sc.width, "height": sc.height, "ms": best,
+                       "geodesics_per_s": n / (best * 1e-3),
+                       "attempts": int(st.attempts), "class_count": [int(x) for x in st.class_count],
+                       "cpu_geodesics_per_s": m / el,
+                       "gpu_over_cpu": (n / (best * 1e-3)) / (m / el),
+                       "cpu_sample": f"{m} seeded samples, {el:.1f} s on {threads} threads"}
+    # the command line end to end: scene, render into host memory, PNG file
+    out = Path(tempfile.mkdtemp()) / "cli.png"
+    argv = ["--disk", "--quiet", "--output", str(out)]
+    import contextlib
+    import io
+    with contextlib.redirect_stdout(io.StringIO()):  # its "Rendered ..." lines
+        for _ in range(warmup):
+            assert cli.main(argv, renderer=r) == 0
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            cli.main(argv, renderer=r)
+        cli_s = (time.perf_counter() - t0) / steps
+    png_bytes = out.stat().st_size
+    out.unlink()
+    n_cli = 800 * 600
+    head = cases["volumetric_disk_schwarzschild"]
+    reasons = sorted({x for c in clk_all for x in c.get("reasons", [])})
+    line = {"metric": "reference CLI render (800x600) geodesics/s per path: volumetric disk, sky map, "
+                      "lensed-spheres scene",
+            "value": head["geodesics_per_s"], "unit": UNIT, "n_gpus": 1, "steps": steps,
+            "warmup": warmup, "ms_per_step": head["ms"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: procedural scenes, seeded 1024x512 sky map",
+            "config": {"workload": "gr_renderer_cli_800x600", "camera": "r=30M, equator, 60 deg FOV",
+                       "stepper": "reference RK45 (FP64 drop-in)", "max_steps": 5000,
+                       "volumetric_disk": "r 6-20 M, scale height 1 M",
+                       "l2": "256 MiB write between timed renders"},
+            "clocks": {"per_case": clk_all, "reasons": reasons},
+            "cases": cases,
+            "cli_png_e2e": {"argv": "gr-renderer --disk (Schwarzschild, 800x600) to a PNG file",
+                            "ms": 1e3 * cli_s, "geodesics_per_s": n_cli / cli_s,
+                            "png_bytes": png_bytes},
+            "gpu_launches": steps * len(cases)}
+    r.close()
+    print(json.dumps(line), flush=True)
+
+
 # ---- reference arm ---------------------------------------------------------------
 def run_reference(args) -> None:
     import numpy as np
@@ -918,11 +1042,12 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["kerr1080p", "stress", "batch", "adjoint"],
+    ap.add_argument("--workload", choices=["kerr1080p", "stress", "batch", "adjoint", "features"],
                     default="kerr1080p",
                     help="stress: the a=0.998 4096^2 x 16 spp configuration (one frame per "
                          "form); batch: 2,048 scenes of uneven size in one launch; adjoint: "
-                         "the 512^2 five-parameter gradient")
+                         "the 512^2 five-parameter gradient; features: the reference CLI render "
+                         "with the volumetric disk, a sky map and the lensed-spheres scene")
     ap.add_argument("--scenes", type=int, default=2048, help="batch: number of scenes")
     ap.add_argument("--split", choices=["frames", "rows"], default="frames",
                     help="kerr1080p with N > 1: one frame per rank (weak scaling, no "
@@ -938,6 +1063,8 @@ def main() -> None:
         run_batch(args)
     elif args.workload == "adjoint":
         run_adjoint(args)
+    elif args.workload == "features":
+        run_features(args)
     else:
         run_ours(args)
 

@@ -46,6 +46,24 @@ def reference_cli(width: int = 800, height: int = 600, metric: str = "schwarzsch
                  RenderOptions(samples_per_axis=samples, sky=ProceduralSky()))
 
 
+def synthetic_sky_map(width: int = 1024, height: int = 512, seed: int = 0):
+    """A seeded equirectangular sky map (height, width, 3) float32 linear RGB
+    standing in for a Radiance file: a blue gradient from the +z pole to a
+    warm horizon band and below it, and 0.2 % of texels as stars of
+    brightness 2-20."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    th = (np.arange(height, dtype=np.float64) + 0.5) / height * math.pi
+    base = np.empty((height, 1, 3))
+    base[:, 0, 0] = 0.15 + 0.55 * np.sin(th) ** 4
+    base[:, 0, 1] = 0.25 + 0.35 * np.sin(th) ** 2
+    base[:, 0, 2] = 0.60 + 0.20 * np.cos(th)
+    px = np.repeat(base, width, axis=1)
+    stars = rng.random((height, width)) < 0.002
+    px[stars] = (2.0 + 18.0 * rng.random((int(stars.sum()), 1))) * np.ones(3)
+    return px.astype(np.float32)
+
+
 def schwarzschild_thin_256(precision: int = abi.GG_PREC_FP64,
                            stepper: int = abi.GG_STEPPER_REFERENCE) -> Scene:
     """Schwarzschild M=1, 256x256, 1 spp, camera r=30 at 80 deg inclination, 60 deg
