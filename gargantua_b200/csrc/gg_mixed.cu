@@ -296,7 +296,7 @@ __global__ void __launch_bounds__(kTraceBlock, MINB)
           n_att = q.n_att;
           n_acc = q.n_acc;
         } else {
-          uint64_t idx = wbase + rank;
+          uint64_t idx = BATCH ? wbase + rank : camera_sample(P, wbase + rank);
           if (BATCH) {
             scene = find_scene(B, idx);
             idx -= B.first[scene];

@@ -165,7 +165,7 @@ __global__ void __launch_bounds__(kTraceBlock,
           n_att = n_att0 = q.n_att;
           n_acc = q.n_acc;
         } else {
-          idx = wbase + rank;
+          idx = camera_sample(P, wbase + rank);
           R = start_sample(P, idx);
           n_att = 0;
           n_acc = 0;

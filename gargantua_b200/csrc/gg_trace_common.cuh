@@ -37,6 +37,27 @@ GG_DEV unsigned lanemask_lt() {
   return m;
 }
 
+// Work order of a camera pass: with GG_CENTER_OUT the traced rows are handed
+// out from the middle outwards (m, m-1, m+1, m-2, ... with m = rows / 2),
+// each row's samples in order; otherwise row by row from the top.  A view of
+// the hole has its costliest rays (the shadow's edge, the photon ring) in the
+// middle; started first, they no longer end a pass alone.  Outputs stay at
+// each sample's own index.  Measured, row order / middle out (ms): the
+// reference CLI's 800 x 600 render with the lensed spheres 17.9 / 15.8, with
+// the volumetric disk 15.9 / 14.6, Kerr with a sky map 26.6 / 24.9; the mixed
+// 1080p Kerr frame 27.7 / 27.4; FP64 1080p and the adjoint unchanged.
+#ifndef GG_CENTER_OUT
+#define GG_CENTER_OUT 1
+#endif
+GG_DEV uint64_t camera_sample(const DevParams& P, uint64_t w) {
+  if (!GG_CENTER_OUT) return w;
+  const uint64_t per_row = (uint64_t)P.width * P.spp;
+  const uint64_t k = w / per_row;
+  const uint64_t m = P.rows / 2;
+  const uint64_t row = (k & 1) ? m - (k + 1) / 2 : m + k / 2;
+  return row * per_row + (w - k * per_row);
+}
+
 // Writes the finished sample's outcome and colour.  Runs once per ray, so it
 // is kept out of line: its shading code (several pow) would otherwise sit in
 // the hot stepping loop's instruction footprint.  (sky_th, sky_ph) is where
