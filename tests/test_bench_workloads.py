@@ -1,0 +1,47 @@
+"""The inputs bench.py times beside the ray path, on the CPU: the seeded sky
+map stands in for a Radiance file, and every case of ``--workload features``
+is a render the oracle (its CPU baseline) can trace."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import bench
+from gargantua_b200 import workloads
+from gargantua_b200.curved import AccretionDisk, HdriSky, ProceduralSky
+
+
+def test_synthetic_sky_map_is_seeded():
+    a = workloads.synthetic_sky_map(64, 32, seed=3)
+    b = workloads.synthetic_sky_map(64, 32, seed=3)
+    c = workloads.synthetic_sky_map(64, 32, seed=4)
+    assert a.shape == (32, 64, 3) and a.dtype == np.float32
+    assert np.array_equal(a, b) and not np.array_equal(a, c)
+    assert np.all(a > 0.0) and np.all(np.isfinite(a))
+    big = workloads.synthetic_sky_map()
+    assert big.shape == (512, 1024, 3)
+    assert 0.001 < (big.max(axis=2) >= 2.0).mean() < 0.004  # the stars
+
+
+def test_feature_cases():
+    cases = bench.feature_scenes()
+    assert list(cases) == ["volumetric_disk_schwarzschild", "volumetric_disk_kerr_a0.9",
+                           "sky_map_kerr_a0.9", "lensed_spheres_schwarzschild",
+                           "lensed_spheres_volumetric_disk_kerr_a0.9"]
+    for name, sc in cases.items():
+        assert (sc.width, sc.height) == (800, 600), name
+        assert isinstance(sc.disk, AccretionDisk) == ("volumetric" in name), name
+        assert (sc.objects is not None) == ("lensed" in name), name
+        sky = sc.options.sky
+        assert isinstance(sky, HdriSky if "sky_map" in name else ProceduralSky), name
+
+
+@pytest.mark.parametrize("name", list(bench.feature_scenes()))
+def test_oracle_traces_each_feature_case(name):
+    from oracle import oracle
+    sc = bench.feature_scenes()[name]
+    idx = np.linspace(0, sc.n_samples - 1, 12).astype(np.uint64)
+    ra = oracle.trace_samples(sc, idx, threads=2)
+    cls = np.asarray(ra.cls)
+    assert np.all((cls >= 0) & (cls <= 5))
+    assert np.all(np.asarray(ra.attempts) > 0)
