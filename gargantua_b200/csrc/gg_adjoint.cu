@@ -58,6 +58,55 @@ GG_DEV void kerr_rhs_dual(double M, const Dual<N>& a, const Dual<N>& r, const Du
   kerr_contract<Dual<N>>(G, w, acc);
 }
 
+// Vector-Jacobian product of one Kerr right-hand side a^mu(r, theta, w; spin)
+// with the cotangent kb: Xr, Xth, W[4] and (accumulated) *ga are kb . da/dr,
+// da/dtheta, da/dw^m and da/dspin.  The geometry depends on (r, theta, spin)
+// only and the contraction is quadratic in w, so the r, theta and spin columns
+// come from a 3-direction dual evaluation with w held constant, and the w
+// columns from a 4-direction dual of the contraction alone with the
+// geometry's values held constant.  Each direction's arithmetic is the one
+// a single 7-direction evaluation would do (the terms dropped are exact
+// zeros), at about half its cost.
+GG_DEV void kerr_rhs_vjp(double M, double spin, double r, double th, const double w[4],
+                         const double kb[4], double* Xr, double* Xth, double W[4], double* ga) {
+  Dual<3> s, c;
+  sincos(Dual<3>::var(th, 1), &s, &c);
+  const KerrGeo<Dual<3>> G =
+      kerr_geometry<Dual<3>>(Dual<3>(M), Dual<3>::var(spin, 2), Dual<3>::var(r, 0), s, c);
+  Dual<3> w3[4], acc3[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) w3[i] = Dual<3>(w[i]);
+  kerr_contract<Dual<3>>(G, w3, acc3);
+  KerrGeo<Dual<4>> Gv;  // the geometry's values, constant in w
+  Gv.dtt_r = G.dtt_r.v;
+  Gv.dtt_th = G.dtt_th.v;
+  Gv.drr_r = G.drr_r.v;
+  Gv.drr_th = G.drr_th.v;
+  Gv.dthth_r = G.dthth_r.v;
+  Gv.dthth_th = G.dthth_th.v;
+  Gv.dphph_r = G.dphph_r.v;
+  Gv.dphph_th = G.dphph_th.v;
+  Gv.dtph_r = G.dtph_r.v;
+  Gv.dtph_th = G.dtph_th.v;
+  Gv.gtt = G.gtt.v;
+  Gv.gtph = G.gtph.v;
+  Gv.gphph = G.gphph.v;
+  Gv.hrr = G.hrr.v;
+  Gv.hthth = G.hthth.v;
+  Dual<4> w4[4], acc4[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) w4[i] = Dual<4>::var(w[i], i);
+  kerr_contract<Dual<4>>(Gv, w4, acc4);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    *Xr += acc3[i].d[0] * kb[i];
+    *Xth += acc3[i].d[1] * kb[i];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) W[m] += acc4[i].d[m] * kb[i];
+    *ga += acc3[i].d[2] * kb[i];
+  }
+}
+
 // g of a Keplerian emitter at the equator (redshift_factor at theta = pi/2)
 // without the observer normalisation (divide by sqrt(-g_tt) at the camera).
 template <class T>
@@ -120,21 +169,9 @@ GG_DEV void dp45_vjp(const DevParams& P, const double x[4], const double v[4], d
 #pragma unroll
     for (int i = 0; i < 4; ++i) kb[l][i] += hh * kDP.Abar[6][l] * lx[i] + h * kDP.B[6][l] * lv[i];
   for (int s = 5; s >= 0; --s) {
-    // k_s = f(r_s, theta_s, w_s; a): its Jacobian from a 7-direction dual
-    Dual<7> w[4], acc[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) w[i] = Dual<7>::var(pw[s][i], 2 + i);
-    kerr_rhs_dual<7>(P.mass, Dual<7>::var(P.spin, 6), Dual<7>::var(pr[s], 0),
-                     Dual<7>::var(pth[s], 1), w, acc);
+    // k_s = f(r_s, theta_s, w_s; a), back through its Jacobian
     double Xr = 0.0, Xth = 0.0, W[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      Xr += acc[i].d[0] * kb[s][i];
-      Xth += acc[i].d[1] * kb[s][i];
-#pragma unroll
-      for (int m = 0; m < 4; ++m) W[m] += acc[i].d[2 + m] * kb[s][i];
-      *ga += acc[i].d[6] * kb[s][i];
-    }
+    kerr_rhs_vjp(P.mass, P.spin, pr[s], pth[s], pw[s], kb[s], &Xr, &Xth, W, ga);
     // x_s = x + h A_s v + h^2 sum_{l<s} Abar k_l ; w_s = v + h sum_{l<s} B k_l
     xbar[1] += Xr;
     xbar[2] += Xth;
