@@ -9,17 +9,24 @@ namespace gg {
 
 constexpr int kTraceBlock = 128;  // threads per CTA of the trace kernels
 
-// Resident CTAs per SM each metric's trace kernel is register-budgeted for
-// (65536 / (128 * blocks) registers per thread).  Kerr's stepping loop hides
-// FP64 latency better with 6 CTAs (80 registers, k vectors in shared
-// memory) despite a few spills; Schwarzschild's lighter right-hand side is
-// fastest at 4.  Measured on B200, Kerr 1920x1080: 4 -> 53.8 ms, 5 -> 50.9
-// ms, 6 -> 49.2 ms.  GG_TRACE_MIN_BLOCKS overrides both (tuning builds).
+// Resident CTAs per SM the FP64 trace kernel is register-budgeted for
+// (65536 / (128 * blocks) registers per thread).  Kerr camera passes: 5 (102
+// registers); Kerr passes set by their longest ray chains -- the mixed form's
+// FP64 band passes, the differentiable render's forward -- 4 (128 registers,
+// no spills on the chain); Schwarzschild's lighter right-hand side: 4.
+// Measured on B200 (ms, CTAs 6 / 5 / 4): FP64 drop-in Kerr 1080p 45.3 /
+// 43.8 / 44.8, its full Dormand-Prince form 59.4 / 55.3 / 55.4, the stress
+// frame at 2048^2 x 4 spp 133.5 / 133.6 / 136.2 (drop-in) and 171.7 / 160.4
+// / 161.9 (full DP); band passes, through the mixed 1080p frame 27.0 / 26.7 /
+// 26.3; the 512^2 adjoint's forward 10.1 / 8.9 / 8.6.  GG_TRACE_MIN_BLOCKS
+// overrides all three (tuning builds).
 #ifdef GG_TRACE_MIN_BLOCKS
 constexpr int kTraceMinBlocksKerr = GG_TRACE_MIN_BLOCKS;
+constexpr int kTraceMinBlocksKerrChain = GG_TRACE_MIN_BLOCKS;
 constexpr int kTraceMinBlocksSchw = GG_TRACE_MIN_BLOCKS;
 #else
-constexpr int kTraceMinBlocksKerr = 6;
+constexpr int kTraceMinBlocksKerr = 5;
+constexpr int kTraceMinBlocksKerrChain = 4;
 constexpr int kTraceMinBlocksSchw = 4;
 #endif
 

@@ -76,7 +76,9 @@ __device__ __noinline__ void hand_back(const DevOutputs& O, DevControl* ctl, Ray
 // survives (O.ckpt) and, when it ends, its DiffRay (O.diff_rays).
 template <int METRIC, int DISK, int STEPPER, int SRC, bool BATCH, bool SCENE, bool CKPT>
 __global__ void __launch_bounds__(kTraceBlock,
-                                  METRIC == kMetricKerr ? kTraceMinBlocksKerr : kTraceMinBlocksSchw)
+                                  METRIC != kMetricKerr        ? kTraceMinBlocksSchw
+                                  : (SRC == kSrcQueue || CKPT) ? kTraceMinBlocksKerrChain
+                                                               : kTraceMinBlocksKerr)
     trace_fp64_kernel(const __grid_constant__ DevParams P, const __grid_constant__ DevOutputs O,
                       DevControl* ctl, const __grid_constant__ BatchTable B) {
   const unsigned lane = threadIdx.x & 31u;
