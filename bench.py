@@ -68,7 +68,7 @@ UNIT = "geodesics/s"
 # frame, measured with ncu (profiles/launches_mixed_kerr_1080p.md): the 6.2 MB
 # image, the band queue and the argument records of the once-per-ray finish
 # and hand-off calls.
-MIXED_PASS_DRAM_BYTES = 3_872_768 + 27_439_360
+MIXED_PASS_DRAM_BYTES = 3_556_864 + 27_299_584
 # Renders of this many samples or more run the mixed form's hand-back rounds
 # (kHandBackMinRays in gargantua_b200/csrc/gg_capi.cpp).
 HAND_BACK_MIN_SAMPLES = 1 << 20

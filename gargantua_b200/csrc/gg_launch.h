@@ -30,11 +30,20 @@ constexpr int kTraceMinBlocksKerrChain = 4;
 constexpr int kTraceMinBlocksSchw = 4;
 #endif
 
-// Resident CTAs per SM the mixed-precision trace kernel is budgeted for.
+// Resident CTAs per SM the mixed-precision trace kernel is budgeted for: its
+// camera pass (8, 64 registers: throughput), and its pass over the rays the
+// FP64 pass hands back (4, 128 registers: set by its longest ray chains).
+// Measured on the 1080p Kerr frame (ms; camera / returned CTAs): 8 / 8 26.4,
+// 7 / 7 26.1, 6 / 6 26.6, 8 / 6 25.9, 8 / 4 25.5, 7 / 4 25.6.
 #ifdef GG_MIXED_MIN_BLOCKS
 constexpr int kMixedMinBlocks = GG_MIXED_MIN_BLOCKS;
 #else
 constexpr int kMixedMinBlocks = 8;
+#endif
+#ifdef GG_MIXED_RET_MIN_BLOCKS
+constexpr int kMixedMinBlocksReturned = GG_MIXED_RET_MIN_BLOCKS;
+#else
+constexpr int kMixedMinBlocksReturned = 4;
 #endif
 
 // Resident CTAs per SM of the trace kernel `P` selects.

@@ -418,7 +418,7 @@ const void* select_mixed_disk(const DevParams& P) {
 // hand-back is off in budgeted renders).
 template <bool BATCH>
 const void* select_returned(const DevParams& P) {
-  constexpr int Pd = kMixedPeriod, Mb = kMixedMinBlocks;
+  constexpr int Pd = kMixedPeriod, Mb = kMixedMinBlocksReturned;
   if (P.metric == kMetricKerr)
     return P.disk == kDiskThin
                ? mixed_fn<kMetricKerr, kDiskThin, false, BATCH, Pd, Mb, kSrcQueue>()
