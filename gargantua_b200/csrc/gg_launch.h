@@ -12,8 +12,9 @@ constexpr int kTraceBlock = 128;  // threads per CTA of the trace kernels
 // Resident CTAs per SM the FP64 trace kernel is register-budgeted for
 // (65536 / (128 * blocks) registers per thread).  Kerr camera passes: 5 (102
 // registers); Kerr passes set by their longest ray chains -- the mixed form's
-// FP64 band passes, the differentiable render's forward -- 4 (128 registers,
-// no spills on the chain); Schwarzschild's lighter right-hand side: 4.
+// FP64 band passes, the differentiable render's forward, camera passes of
+// fewer than 2^20 samples -- 4 (128 registers, no spills on the chain);
+// Schwarzschild's lighter right-hand side: 4.
 // Measured on B200 (ms, CTAs 6 / 5 / 4): FP64 drop-in Kerr 1080p 45.3 /
 // 43.8 / 44.8, its full Dormand-Prince form 59.4 / 55.3 / 55.4, the stress
 // frame at 2048^2 x 4 spp 133.5 / 133.6 / 136.2 (drop-in) and 171.7 / 160.4

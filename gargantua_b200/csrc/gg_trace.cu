@@ -74,11 +74,12 @@ __device__ __noinline__ void hand_back(const DevOutputs& O, DevControl* ctl, Ray
 // the differentiable render's forward, which also stores each ray's state
 // (x, v, next h) at its start and after every kCkptEvery-th accepted step it
 // survives (O.ckpt) and, when it ends, its DiffRay (O.diff_rays).
-template <int METRIC, int DISK, int STEPPER, int SRC, bool BATCH, bool SCENE, bool CKPT>
+template <int METRIC, int DISK, int STEPPER, int SRC, bool BATCH, bool SCENE, bool CKPT,
+          bool SMALL>
 __global__ void __launch_bounds__(kTraceBlock,
-                                  METRIC != kMetricKerr        ? kTraceMinBlocksSchw
-                                  : (SRC == kSrcQueue || CKPT) ? kTraceMinBlocksKerrChain
-                                                               : kTraceMinBlocksKerr)
+                                  METRIC != kMetricKerr                 ? kTraceMinBlocksSchw
+                                  : (SRC == kSrcQueue || CKPT || SMALL) ? kTraceMinBlocksKerrChain
+                                                                        : kTraceMinBlocksKerr)
     trace_fp64_kernel(const __grid_constant__ DevParams P, const __grid_constant__ DevOutputs O,
                       DevControl* ctl, const __grid_constant__ BatchTable B) {
   const unsigned lane = threadIdx.x & 31u;
@@ -481,34 +482,52 @@ __global__ void reduce_samples_kernel(const __grid_constant__ DevParams P, const
 }
 
 template <int METRIC, int DISK, int STEPPER, int SRC, bool BATCH = false, bool SCENE = false,
-          bool CKPT = false>
+          bool CKPT = false, bool SMALL = false>
 const void* trace_fn() {
   return reinterpret_cast<const void*>(
-      &trace_fp64_kernel<METRIC, DISK, STEPPER, SRC, BATCH, SCENE, CKPT>);
+      &trace_fp64_kernel<METRIC, DISK, STEPPER, SRC, BATCH, SCENE, CKPT, SMALL>);
 }
+
+// Kerr camera passes of fewer samples than this run the 4-CTA budget of the
+// chain-bound passes: a few rays per lane, so the longest rays set the time.
+constexpr uint64_t kSmallRender = 1ull << 20;
 
 // With a scene: no disk or the volumetric one (the reference's
 // render_with_scene and render_with_disk_and_scene).
+template <int STEPPER, bool SMALL>
+const void* select_scene_kerr(const DevParams& P) {
+  return P.disk == kDiskVolumetric
+             ? trace_fn<kMetricKerr, kDiskVolumetric, STEPPER, kSrcCamera, false, true, false,
+                        SMALL>()
+             : trace_fn<kMetricKerr, kDiskNone, STEPPER, kSrcCamera, false, true, false, SMALL>();
+}
+
 template <int STEPPER>
 const void* select_scene(const DevParams& P) {
   if (P.metric == kMetricKerr)
-    return P.disk == kDiskVolumetric
-               ? trace_fn<kMetricKerr, kDiskVolumetric, STEPPER, kSrcCamera, false, true>()
-               : trace_fn<kMetricKerr, kDiskNone, STEPPER, kSrcCamera, false, true>();
+    return P.n_rays < kSmallRender ? select_scene_kerr<STEPPER, true>(P)
+                                   : select_scene_kerr<STEPPER, false>(P);
   return P.disk == kDiskVolumetric
              ? trace_fn<kMetricSchwarzschild, kDiskVolumetric, STEPPER, kSrcCamera, false, true>()
              : trace_fn<kMetricSchwarzschild, kDiskNone, STEPPER, kSrcCamera, false, true>();
 }
 
+template <int STEPPER, bool SMALL>
+const void* select_disk_kerr(const DevParams& P) {
+  if (P.disk == kDiskThin)
+    return trace_fn<kMetricKerr, kDiskThin, STEPPER, kSrcCamera, false, false, false, SMALL>();
+  if (P.disk == kDiskVolumetric)
+    return trace_fn<kMetricKerr, kDiskVolumetric, STEPPER, kSrcCamera, false, false, false,
+                    SMALL>();
+  return trace_fn<kMetricKerr, kDiskNone, STEPPER, kSrcCamera, false, false, false, SMALL>();
+}
+
 template <int STEPPER>
 const void* select_metric_disk(const DevParams& P) {
   if (P.scene) return select_scene<STEPPER>(P);
-  if (P.metric == kMetricKerr) {
-    if (P.disk == kDiskThin) return trace_fn<kMetricKerr, kDiskThin, STEPPER, kSrcCamera>();
-    if (P.disk == kDiskVolumetric)
-      return trace_fn<kMetricKerr, kDiskVolumetric, STEPPER, kSrcCamera>();
-    return trace_fn<kMetricKerr, kDiskNone, STEPPER, kSrcCamera>();
-  }
+  if (P.metric == kMetricKerr)
+    return P.n_rays < kSmallRender ? select_disk_kerr<STEPPER, true>(P)
+                                   : select_disk_kerr<STEPPER, false>(P);
   if (P.disk == kDiskThin) return trace_fn<kMetricSchwarzschild, kDiskThin, STEPPER, kSrcCamera>();
   if (P.disk == kDiskVolumetric)
     return trace_fn<kMetricSchwarzschild, kDiskVolumetric, STEPPER, kSrcCamera>();
