@@ -19,15 +19,22 @@ constexpr int kTraceBlock = 128;  // threads per CTA of the trace kernels
 // 43.8 / 44.8, its full Dormand-Prince form 59.4 / 55.3 / 55.4, the stress
 // frame at 2048^2 x 4 spp 133.5 / 133.6 / 136.2 (drop-in) and 171.7 / 160.4
 // / 161.9 (full DP); band passes, through the mixed 1080p frame 27.0 / 26.7 /
-// 26.3; the 512^2 adjoint's forward 10.1 / 8.9 / 8.6.  GG_TRACE_MIN_BLOCKS
-// overrides all three (tuning builds).
+// 26.3; the 512^2 adjoint's forward 10.1 / 8.9 / 8.6.  At 3 CTAs (168
+// registers) for the band passes and the mixed pass over returned rays, the
+// 1080p frame gains 0.3 ms but the stress frame at 2048^2 x 4 spp, whose band
+// holds 12 % of the attempts, loses 1.3 ms.  GG_TRACE_MIN_BLOCKS overrides
+// all three, GG_TRACE_CHAIN_MIN_BLOCKS the chain-bound one (tuning builds).
 #ifdef GG_TRACE_MIN_BLOCKS
 constexpr int kTraceMinBlocksKerr = GG_TRACE_MIN_BLOCKS;
 constexpr int kTraceMinBlocksKerrChain = GG_TRACE_MIN_BLOCKS;
 constexpr int kTraceMinBlocksSchw = GG_TRACE_MIN_BLOCKS;
 #else
 constexpr int kTraceMinBlocksKerr = 5;
+#ifdef GG_TRACE_CHAIN_MIN_BLOCKS
+constexpr int kTraceMinBlocksKerrChain = GG_TRACE_CHAIN_MIN_BLOCKS;
+#else
 constexpr int kTraceMinBlocksKerrChain = 4;
+#endif
 constexpr int kTraceMinBlocksSchw = 4;
 #endif
 
