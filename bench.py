@@ -633,7 +633,7 @@ def run_batch(args) -> None:
             "rays": rays, "attempts": attempts, "attempts_per_s": attempts / (best * 1e-3),
             "fp64_band_rays": band_rays, "fp64_band_attempts": band_att,
             "autotune": {"variant": variant, "variant_ms_on_every_8th_scene": tune_ms,
-                         "variants": "0..5 = (period, CTAs/SM) (16,8) (8,8) (4,8) (16,7) (8,7) (4,7)",
+                         "variants": "0..5 = (period, CTAs/SM) (16,8) (8,8) (4,8) (16,7) (32,7) (32,8)",
                          "wall_s": tune_s}}
     if world == 1:
         line["class_count"] = [int(x) for x in st.class_count]

@@ -437,8 +437,8 @@ const void* batch_variant(int v) {
     case 1: return mixed_fn<METRIC, DISK, false, true, 8, 8>();
     case 2: return mixed_fn<METRIC, DISK, false, true, 4, 8>();
     case 3: return mixed_fn<METRIC, DISK, false, true, 16, 7>();
-    case 4: return mixed_fn<METRIC, DISK, false, true, 8, 7>();
-    default: return mixed_fn<METRIC, DISK, false, true, 4, 7>();
+    case 4: return mixed_fn<METRIC, DISK, false, true, 32, 7>();
+    default: return mixed_fn<METRIC, DISK, false, true, 32, 8>();
   }
 }
 
