@@ -46,6 +46,27 @@ def test_row_shards_partition_the_image(height, world):
     assert all(x.width == s.width and x.max_steps == s.max_steps for x in shards)
 
 
+@pytest.mark.parametrize("rank,world", [(0, 1), (1, 3)])
+def test_scene_at_is_the_forward_render(rank, world):
+    """DiffScene.scene_at(p) passes the C ABI the same metric, disk,
+    integrator, options and camera as the differentiable forward does: the
+    bench takes the forward's attempt count and the oracle's baseline from it."""
+    import ctypes as C
+    s = diff.DiffScene(width=64, height=48).shard(rank, world)
+    p = diff.perturbed_params()
+    # DiffRenderer() opens a GPU context; its struct builder needs only .scene
+    m, d, integ, opts, incl, r_cam = diff.DiffRenderer._structs(
+        type("DR", (), {"scene": s})(), p)
+    m2, cam2, d2, integ2, opts2 = s.scene_at(p).c_structs()
+    for a, b in ((m, m2), (d, d2), (integ, integ2), (opts, opts2)):
+        assert C.string_at(C.addressof(a), C.sizeof(a)) == C.string_at(C.addressof(b), C.sizeof(b))
+    cam = abi.gg_camera_t()
+    abi.check(abi.load().gg_camera_inclined(C.byref(cam), r_cam, incl, s.fov_y,
+                                            s.width / s.height), "gg_camera_inclined")
+    assert C.string_at(C.addressof(cam), C.sizeof(cam)) == C.string_at(C.addressof(cam2),
+                                                                       C.sizeof(cam2))
+
+
 def _allreduce_worker(rank, world, port, q):
     import torch.distributed as dist
     os.environ["MASTER_ADDR"] = "127.0.0.1"
