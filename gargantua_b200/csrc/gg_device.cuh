@@ -407,9 +407,13 @@ GG_DEV int attempt_fp64(const DevParams& P, Ray& R, const KStore& K, bool& k1_va
   // inputs and the k registers are selected per stage by switch arms
   // (warp-uniform branches; all lanes of a warp run the same stage).  The
   // last pass evaluates k6 and k7, which share the position pos6.
-  // Warp-uniform first stage: a lane whose k1 is valid recomputes the same
-  // value when a refilled lane in its warp needs k1, instead of the warp
-  // running the whole attempt diverged.
+  // Warp-uniform first stage: when a refilled lane in the warp needs k1, the
+  // whole warp runs stage 0 instead of the attempt diverged, but a lane whose
+  // k1 is valid keeps its own (the previous step's k7).  k7 is evaluated at
+  // another call site of the contraction, which the compiler may fuse into
+  // multiply-adds differently, so a recomputed k1 can differ from it in the
+  // last bit; overwriting it would make a ray's result depend on which rays
+  // share its warp.
   const int s_first = __any_sync(__activemask(), !k1_valid) ? 0 : 1;
 #pragma unroll 1
   for (int s = s_first; s < 6; ++s) {
@@ -456,8 +460,11 @@ GG_DEV int attempt_fp64(const DevParams& P, Ray& R, const KStore& K, bool& k1_va
     G.accel(w, a);
     switch (s) {
       case 0:
+        if (!k1_valid) {
 #pragma unroll
-        for (int i = 0; i < 4; ++i) K(0, i) = a[i];
+          for (int i = 0; i < 4; ++i) K(0, i) = a[i];
+          k1_valid = true;  // a rejected attempt leaves the state, so k1 stays
+        }
         break;
       case 1:
 #pragma unroll
@@ -993,9 +1000,9 @@ GG_DEV void hdri_sky(const DevParams& P, const double v[4], double rgb[3]) {
   }
 }
 
-GG_DEV void procedural_sky(const double v[4], double rgb[3]) {
-  double d0, d1, d2;
-  spatial_dir(v, d0, d1, d2);
+// ProceduralSky::sample (sky.rs:26-40) of a unit direction (d0, d1, d2):
+// the hash of the directions' f64 bits picks stars, else a blue gradient.
+GG_DEV void procedural_sky_dir(double d0, double d1, double d2, double rgb[3]) {
   auto hash = [](double x) -> uint64_t {
     return (uint64_t)__double_as_longlong(x) * 6364136223846793005ULL +
            1442695040888963407ULL;
@@ -1011,6 +1018,14 @@ GG_DEV void procedural_sky(const double v[4], double rgb[3]) {
     rgb[1] = 0.0;
     rgb[2] = add_rn(10.0 / 255.0, vv);
   }
+}
+
+// The starfield seen along an escaped ray's final velocity (tracer.rs:185-189
+// then sky.rs:26-40).
+GG_DEV void procedural_sky(const double v[4], double rgb[3]) {
+  double d0, d1, d2;
+  spatial_dir(v, d0, d1, d2);
+  procedural_sky_dir(d0, d1, d2, rgb);
 }
 
 // Seeded checkerboard over the escape point's (theta, phi).
