@@ -19,7 +19,6 @@
 
 #include <cstdint>
 #include <cstring>
-#include <mutex>
 
 #include "../../include/gargantua_gpu.h"
 #include "gg_host.h"
@@ -36,25 +35,29 @@ constexpr uint64_t kMaxSupersampled = (kScratchBytes - kControlBytes) / (3 * siz
 
 __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
-// Device address of g_noalloc_scratch per device ordinal.  In host code the
-// symbol is only a host-side handle, so each device's address is looked up
-// once, with that device current, and cached.
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-void* g_scratch_addr[kMaxDevices];
-
-int scratch_address(int device, void** out) {
-  std::lock_guard<std::mutex> lock(g_mu);
-  if (!g_scratch_addr[device]) {
-    void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
-      cudaGetLastError();
-      return GG_ERR_CUDA;
-    }
-    g_scratch_addr[device] = p;
+// Device address of g_noalloc_scratch in the current device's context.  In
+// host code the symbol is only a host-side handle.  The address is looked up
+// on every call, with the device current, and not cached: after a
+// cudaDeviceReset the module is reloaded and the array may move, and another
+// context on the same device holds its own copy of the array.  Once the
+// module is loaded in a context the lookup allocates nothing; the first call
+// on a device loads it there.
+int scratch_address(void** out) {
+  void* p = nullptr;
+  if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
+    cudaGetLastError();
+    return GG_ERR_CUDA;
   }
-  *out = g_scratch_addr[device];
+  *out = p;
   return GG_OK;
+}
+
+// A failed runtime call's error code stays as the thread's last error, where
+// a later successful call (which checks cudaGetLastError after its launches)
+// would find it: clear it before reporting the failure.
+int cuda_failed() {
+  cudaGetLastError();
+  return GG_ERR_CUDA;
 }
 
 }  // namespace
@@ -82,14 +85,13 @@ extern "C" GG_API int gg_render_device_noalloc(const gg_metric_t* metric,
     cudaGetLastError();
     return GG_ERR_NO_DEVICE;
   }
-  if (device < 0 || device >= kMaxDevices) return GG_ERR_UNSUPPORTED;
   int major = 0, sms = 0;
   if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device) != cudaSuccess ||
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
-    return GG_ERR_CUDA;
+    return cuda_failed();
   if (major != 10) return GG_ERR_NO_DEVICE;
   void* base = nullptr;
-  const int st = scratch_address(device, &base);
+  const int st = scratch_address(&base);
   if (st != GG_OK) return st;
 
   gg::DevControl* ctl = static_cast<gg::DevControl*>(base);
@@ -113,15 +115,15 @@ extern "C" GG_API int gg_render_device_noalloc(const gg_metric_t* metric,
 
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   // the counters keep the previous call's totals: the work queue must start at 0
-  if (cudaMemsetAsync(ctl, 0, sizeof(gg::DevControl), s) != cudaSuccess) return GG_ERR_CUDA;
+  if (cudaMemsetAsync(ctl, 0, sizeof(gg::DevControl), s) != cudaSuccess) return cuda_failed();
   int bps = 0;
-  if (gg::trace_occupancy(P, &bps) != cudaSuccess || bps < 1) return GG_ERR_CUDA;
+  if (gg::trace_occupancy(P, &bps) != cudaSuccess || bps < 1) return cuda_failed();
   uint64_t grid = (uint64_t)sms * (uint64_t)bps;
   const uint64_t need_blocks = (P.n_rays + gg::kTraceBlock - 1) / gg::kTraceBlock;
   if (grid > need_blocks) grid = need_blocks;
   if (grid < 1) grid = 1;
-  if (gg::launch_trace(P, O, ctl, (int)grid, s) != cudaSuccess) return GG_ERR_CUDA;
+  if (gg::launch_trace(P, O, ctl, (int)grid, s) != cudaSuccess) return cuda_failed();
   if (need_samples && gg::launch_reduce(P, O.sample_rgb, rgb_dev, sms, s) != cudaSuccess)
-    return GG_ERR_CUDA;
+    return cuda_failed();
   return GG_OK;
 }

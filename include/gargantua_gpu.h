@@ -255,8 +255,11 @@ GG_API int gg_render_device(gg_ctx* ctx, const gg_metric_t* metric, const gg_cam
  *   - Supersampled images are limited to 699,040 samples
  *     (width * height * spp); larger ones return GG_ERR_TOO_LARGE.
  *     Single-sample images have no size limit here.
- *   - The first call on a device looks up the array's device address (once
- *     per device); make that first call before any stream capture.
+ *   - Every call looks up the array's device address in the current
+ *     context, so the entry point stays valid after cudaDeviceReset and
+ *     under any context.  The first call on a device also loads this
+ *     library's device code there: make that first call before any stream
+ *     capture.
  *   - Every call on a device shares the one array: calls whose work overlaps
  *     on the GPU (different streams, not ordered) race and corrupt each
  *     other's results.  Order them, for example on one stream.
@@ -396,6 +399,19 @@ GG_API int gg_measure_fma_peak(gg_ctx* ctx, int fp64, double* flops);
  * host from the same source so its accuracy can be checked without a GPU.
  * 0, or -1 for a NULL pointer.  No reference counterpart. */
 GG_API int gg_polar_sincos(const float* theta, float* s, float* c, uint32_t n);
+
+/* Device functions exported for bit-exact checks against the oracle on
+ * identical inputs (test use; no reference counterpart).  Device pointers,
+ * enqueued on `stream` (NULL = CUDA's default stream); 0, GG_ERR_INVALID_ARG
+ * for a NULL pointer, GG_ERR_CUDA if the launch failed.
+ * gg_check_procedural_sky: ProceduralSky::sample (sky.rs:26-40) of n unit
+ *   directions dirs[3 i .. 3 i + 2] into rgb[3 i .. 3 i + 2].
+ * gg_check_spatial_dir: spatial_dir (tracer.rs:185-189) of n velocities
+ *   vel[4 i .. 4 i + 3] into dirs[3 i .. 3 i + 2]. */
+GG_API int gg_check_procedural_sky(const double* dirs_dev, double* rgb_dev, uint64_t n,
+                                   void* stream);
+GG_API int gg_check_spatial_dir(const double* vel_dev, double* dirs_dev, uint64_t n,
+                                void* stream);
 
 #ifdef __cplusplus
 }

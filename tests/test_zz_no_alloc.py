@@ -21,7 +21,8 @@ from gargantua_b200.curved import RayOutputs, Renderer
 
 pytestmark = pytest.mark.gpu
 
-FIELDS = ("cls", "x", "v", "lam", "attempts", "accepted", "intensity", "rgb", "cross")
+FIELDS = ("cls", "x", "v", "lam", "attempts", "accepted", "intensity", "color_temp", "rgb",
+          "cross")
 
 
 def device_rays(torch, n):
@@ -67,6 +68,7 @@ def noalloc_render(torch, scene):
     out.attempts = rays["attempts"].cpu().numpy().view(np.uint32)
     out.accepted = rays["accepted"].cpu().numpy().view(np.uint32)
     out.intensity = rays["intensity"].cpu().numpy()
+    out.color_temp = rays["color_temp"].cpu().numpy()
     out.rgb = rays["rgb"].cpu().numpy().reshape(n, 3)
     out.cross = rays["cross"].cpu().numpy().reshape(8, n)
     return img, out
@@ -119,12 +121,52 @@ def test_noalloc_kerr_scene_matches(torch_cuda):
     same(got, want)
 
 
-def test_noalloc_rejects_oversized_supersampling(torch_cuda):
+def test_noalloc_supersampling_at_the_scratch_limit(torch_cuda):
+    # 680 x 257 pixels x 4 samples = 699,040, the last sample's colour ending
+    # exactly at the end of the array
     scene = workloads.schwarzschild_thin_256()
-    scene.width = scene.height = 1024
-    scene.options.samples_per_axis = 2  # 4,194,304 samples > 699,040
+    scene.width, scene.height = 680, 257
+    scene.options.samples_per_axis = 2
+    assert scene.n_samples == 699040
+    r = Renderer(0)
+    try:
+        want_img, want = r.render(scene, rays=True)
+    finally:
+        r.close()
+    img, got = noalloc_render(torch_cuda, scene)
+    assert np.array_equal(img, want_img)
+    same(got, want)
+
+
+def test_noalloc_second_call_allocates_nothing(torch_cuda):
+    # after a first call has loaded the module on this device, a call leaves
+    # the device's free memory exactly as it was
+    scene = workloads.schwarzschild_thin_256()
+    scene.width = scene.height = 64
+    scene.options.samples_per_axis = 2
+    noalloc_render(torch_cuda, scene)
+    lib = abi.load()
+    rgb = torch_cuda.zeros(scene.width * scene.height * 3, dtype=torch_cuda.uint8, device="cuda")
+    torch_cuda.cuda.synchronize()
+    free0, _ = torch_cuda.cuda.mem_get_info()
+    st = lib.gg_render_device_noalloc(*scene.c_args(), C.c_void_p(rgb.data_ptr()), None, None)
+    torch_cuda.cuda.synchronize()
+    free1, _ = torch_cuda.cuda.mem_get_info()
+    assert st == abi.GG_OK
+    assert free1 == free0
+
+
+@pytest.mark.parametrize("shape", [(1024, 1024, 2, 0), (2699, 37, 1, 7)],
+                         ids=["4M-samples", "one-past-the-limit"])
+def test_noalloc_rejects_oversized_supersampling(torch_cuda, shape):
+    w, h, spa, jitter = shape
+    scene = workloads.schwarzschild_thin_256()
+    scene.width, scene.height = w, h
+    scene.options.samples_per_axis = spa
+    scene.options.jitter_spp = jitter
+    assert scene.n_samples in (4194304, 699041)
     rgb = torch_cuda.zeros(16, dtype=torch_cuda.uint8, device="cuda")
-    st = abi.load().gg_render_device_noalloc(*scene.c_args(), C.c_void_p(rgb.data_ptr()),
-                                             None, None)
+    lib = abi.load()
+    st = lib.gg_render_device_noalloc(*scene.c_args(), C.c_void_p(rgb.data_ptr()), None, None)
     assert st == abi.GG_ERR_TOO_LARGE
-    assert b"scratch" in abi.load().gg_strerror(st)
+    assert b"scratch" in lib.gg_strerror(st)
