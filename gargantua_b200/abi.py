@@ -154,6 +154,8 @@ _SIGNATURES = {
                                    C.c_uint32, C.c_void_p, P(gg_ray_out_t), C.c_void_p]),
     "gg_measure_fma_peak": (C.c_int, [C.c_void_p, C.c_int, P(C.c_double)]),
     "gg_polar_sincos": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32]),
+    "gg_check_procedural_sky": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p]),
+    "gg_check_spatial_dir": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p]),
     "gg_render_batch": (C.c_int, [C.c_void_p, P(gg_scene_t), C.c_uint32, P(gg_integrator_t),
                                   P(gg_render_opts_t), C.c_void_p]),
     "gg_render_batch_device": (C.c_int, [C.c_void_p, P(gg_scene_t), C.c_uint32,

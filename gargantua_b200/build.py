@@ -20,7 +20,7 @@ PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 OUT = PKG / "libgargantua_gpu.so"
 SOURCES = ["gg_trace.cu", "gg_mixed.cu", "gg_adjoint.cu", "gg_peak.cu", "gg_capi.cpp",
-           "gg_scene_build.cpp", "gg_noalloc.cu"]
+           "gg_scene_build.cpp", "gg_noalloc.cu", "gg_checks.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -398,6 +398,18 @@ GGO_API int ggo_from_camera(const gg_metric_t* m, const gg_camera_t* camera, uin
   });
 }
 
+// ggo_from_camera for n pixel centres, pixel index i = py * w + px in
+// index[k], state k in states[9 k .. 9 k + 8].
+GGO_API int ggo_from_camera_n(const gg_metric_t* m, const gg_camera_t* camera, uint32_t w,
+                              uint32_t h, const uint64_t* index, uint64_t n, double* states) {
+  for (uint64_t k = 0; k < n; ++k) {
+    const int st = ggo_from_camera(m, camera, (uint32_t)(index[k] % w), (uint32_t)(index[k] / w),
+                                   w, h, states + 9 * k);
+    if (st != 0) return st;
+  }
+  return 0;
+}
+
 GGO_API double ggo_redshift_factor(const gg_metric_t* m, const double pos[4], const double p[4],
                                    double sqrt_neg_gtt_obs) {
   double g = 0.0;
@@ -411,6 +423,24 @@ GGO_API double ggo_redshift_factor(const gg_metric_t* m, const double pos[4], co
 
 GGO_API void ggo_procedural_sky(const double dir[3], double rgb[3]) {
   procedural_sky(V3{{dir[0], dir[1], dir[2]}}, rgb);
+}
+
+// spatial_dir (tracer.rs:185-189) of a velocity 4-vector.
+GGO_API void ggo_spatial_dir(const double v[4], double dir[3]) {
+  const V3 d = spatial_dir(V4<double>{{v[0], v[1], v[2], v[3]}});
+  dir[0] = d[0];
+  dir[1] = d[1];
+  dir[2] = d[2];
+}
+
+// Batched forms of the two above over n inputs (rows of 3 and 4 doubles).
+GGO_API void ggo_procedural_sky_n(const double* dirs, double* rgb, uint64_t n) {
+  for (uint64_t i = 0; i < n; ++i)
+    procedural_sky(V3{{dirs[3 * i], dirs[3 * i + 1], dirs[3 * i + 2]}}, rgb + 3 * i);
+}
+
+GGO_API void ggo_spatial_dir_n(const double* v, double* dirs, uint64_t n) {
+  for (uint64_t i = 0; i < n; ++i) ggo_spatial_dir(v + 4 * i, dirs + 3 * i);
 }
 
 GGO_API void ggo_checker_sky(double theta, double phi, uint32_t rows, uint32_t cols,

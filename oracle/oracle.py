@@ -77,6 +77,11 @@ def lib(variant: str = "plain") -> C.CDLL:
             "ggo_redshift_factor": (C.c_double, [P(abi.gg_metric_t), C.c_void_p, C.c_void_p,
                                                  C.c_double]),
             "ggo_procedural_sky": (None, [C.c_void_p, C.c_void_p]),
+            "ggo_spatial_dir": (None, [C.c_void_p, C.c_void_p]),
+            "ggo_procedural_sky_n": (None, [C.c_void_p, C.c_void_p, C.c_uint64]),
+            "ggo_from_camera_n": (C.c_int, [P(abi.gg_metric_t), P(abi.gg_camera_t), C.c_uint32,
+                                            C.c_uint32, C.c_void_p, C.c_uint64, C.c_void_p]),
+            "ggo_spatial_dir_n": (None, [C.c_void_p, C.c_void_p, C.c_uint64]),
             "ggo_checker_sky": (None, [C.c_double, C.c_double, C.c_uint32, C.c_uint32,
                                        C.c_uint64, C.c_void_p]),
             "ggo_disk_color": (None, [C.c_double, C.c_void_p]),
@@ -216,3 +221,56 @@ def trace_cross(scene, index: np.ndarray, threads: int = 0) -> np.ndarray:
     st = lib().ggo_trace_cross(*scene.c_args(), _ptr(index), len(index), _ptr(out), threads)
     abi.check(st, "ggo_trace_cross")
     return out
+
+
+def kerr_thin_1080p():
+    """The Kerr a = 0.9 1920x1080 thin-disk frame (camera r = 50 M at 75 deg,
+    60 deg FOV, disk r_ISCO-30 M with q = 3, 18x36 checkerboard sky seed 0,
+    the reference's RK45 step with rtol 1e-8 / atol 1e-10, 10,000 step()
+    calls, escape at 200 M), built from the oracle alone: the ISCO from
+    ``ggo_kerr_isco`` and the camera frame written out here, so that timing
+    the oracle on it maps none of the product's native code.  Field for field
+    the scene ``gargantua_b200.workloads.kerr_thin_1080p()`` builds (a test
+    checks that)."""
+    import math
+
+    from gargantua_b200.curved import Camera, CheckerSky, RenderOptions, Scene, ThinDisk
+    from gargantua_b200.gr_core import Kerr, RK45Integrator
+
+    k = Kerr(1.0, 0.9)
+    incl = math.radians(75.0)
+    cam = Camera((0.0, 50.0, incl, 0.0), (-math.sin(incl), 0.0, -math.cos(incl)),
+                 (0.0, 0.0, 1.0), math.radians(60.0), 1920 / 1080)
+    integ = RK45Integrator(max_radius=200.0, rtol=1e-8, atol=1e-10)
+    return Scene(k, cam, 1920, 1080, ThinDisk(lib().ggo_kerr_isco(k.mass, k.spin), 30.0, 3.0),
+                 RenderOptions(sky=CheckerSky(18, 36, 0), max_steps=10000, integrator=integ))
+
+
+def procedural_sky_n(dirs: np.ndarray) -> np.ndarray:
+    """ProceduralSky::sample (sky.rs:26-40) of n directions (n x 3) -> n x 3."""
+    d = np.ascontiguousarray(dirs, np.float64)
+    out = np.zeros_like(d)
+    lib().ggo_procedural_sky_n(_ptr(d), _ptr(out), len(d))
+    return out
+
+
+def spatial_dir_n(vel: np.ndarray) -> np.ndarray:
+    """spatial_dir (tracer.rs:185-189) of n velocities (n x 4) -> n x 3."""
+    v = np.ascontiguousarray(vel, np.float64)
+    out = np.zeros((len(v), 3))
+    lib().ggo_spatial_dir_n(_ptr(v), _ptr(out), len(v))
+    return out
+
+
+def initial_states(scene, index: np.ndarray | None = None) -> tuple[np.ndarray, np.ndarray]:
+    """GeodesicRay::from_camera (ray.rs:14-61) at the centres of pixels
+    `index` (py * width + px; default all): positions and velocities, 4 x n
+    each."""
+    idx = np.arange(scene.width * scene.height, dtype=np.uint64) if index is None else \
+        np.ascontiguousarray(index, np.uint64)
+    st = np.zeros((len(idx), 9))
+    m, c = scene.metric.to_c(), scene.camera.to_c()
+    r = lib().ggo_from_camera_n(C.byref(m), C.byref(c), scene.width, scene.height, _ptr(idx),
+                                len(idx), _ptr(st))
+    abi.check(r, "ggo_from_camera_n")
+    return st[:, :4].T.copy(), st[:, 4:8].T.copy()
