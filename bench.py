@@ -65,9 +65,9 @@ sys.path.insert(0, str(ROOT))
 METRIC = "Kerr 1080p geodesics/s, mixed-FP32 vs plain FP64 on B200 at stated endpoint error"
 UNIT = "geodesics/s"
 # DRAM bytes (read + write) of one launch of the FP32 pass on the Kerr 1080p
-# frame, measured with ncu (profiles/launches_mixed_kerr_1080p.md): the 6.2 MB
-# image, the band queue and the argument records of the once-per-ray finish
-# and hand-off calls.
+# frame: ncu's dram__bytes_read.sum + dram__bytes_write.sum for that launch
+# (one pass, clocks not locked).  They are the 6.2 MB image, the band queue and
+# the argument records of the once-per-ray finish and hand-off calls.
 MIXED_PASS_DRAM_BYTES = 3_556_864 + 27_299_584
 # Renders of this many samples or more run the mixed form's hand-back rounds
 # (kHandBackMinRays in gargantua_b200/csrc/gg_capi.cpp).
@@ -423,7 +423,7 @@ def run_ours(args) -> None:
         "roofline": {"bound": "fp32", "achieved": achieved / 1e12,
                      "peak": peak / 1e12, "unit": "TFLOP/s", "frac": achieved / peak,
                      # DRAM read + write of the FP32 pass, one launch of this frame
-                     # (ncu dram__bytes_{read,write}.sum; profiles/launches_mixed_kerr_1080p.md)
+                     # (ncu dram__bytes_{read,write}.sum of that launch)
                      "traffic": MIXED_PASS_DRAM_BYTES,
                      "traffic_unit": "bytes per launch of trace_mixed_kernel",
                      "kernel": "trace_mixed_kernel<Kerr, ThinDisk> + FP64 band pass",
@@ -991,16 +991,31 @@ def run_features(args) -> None:
 
 
 # ---- reference arm ---------------------------------------------------------------
+def native_libraries() -> list[str]:
+    """Shared objects under this repository mapped into this process."""
+    found = set()
+    try:
+        with open("/proc/self/maps") as f:
+            for line in f:
+                path = line.split()[-1] if len(line.split()) >= 6 else ""
+                if path.endswith(".so") and path.startswith(str(ROOT)):
+                    found.add(os.path.relpath(path, ROOT))
+    except OSError:
+        pass
+    return sorted(found)
+
+
 def run_reference(args) -> None:
     import numpy as np
 
-    from gargantua_b200 import workloads
     from oracle import oracle
 
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    scene = workloads.kerr_thin_1080p()
+    # the scene from the oracle alone: this arm maps none of the product's
+    # native code (the line lists what it mapped)
+    scene = oracle.kerr_thin_1080p()
     threads = len(os.sched_getaffinity(0))
     rng = np.random.default_rng(0)
     probe = np.sort(rng.choice(scene.n_samples, 2048, replace=False)).astype(np.uint64)
@@ -1008,8 +1023,8 @@ def run_reference(args) -> None:
     oracle.trace_samples(scene, probe, threads=threads)
     rate = 2048 / (time.perf_counter() - t0)
     steps, warmup = args.steps, max(3, args.warmup)
-    per_step_s = min(20.0, 150.0 / (steps + warmup))
-    n = int(min(scene.n_samples, max(2048, rate * per_step_s)))
+    per_step_s = args.ref_step_s or min(20.0, 150.0 / (steps + warmup))
+    n = int(min(scene.n_samples, max(256, rate * per_step_s)))
     idx = np.sort(rng.choice(scene.n_samples, n, replace=False)).astype(np.uint64)
     for _ in range(warmup):
         oracle.trace_samples(scene, idx[: max(256, n // 8)], threads=threads)
@@ -1031,7 +1046,8 @@ def run_reference(args) -> None:
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                              "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}
+                    "d2h_bytes_per_step": 0},
+            "native_so_loaded": native_libraries()}
     print(json.dumps(line), flush=True)
 
 
@@ -1052,6 +1068,9 @@ def main() -> None:
     ap.add_argument("--split", choices=["frames", "rows"], default="frames",
                     help="kerr1080p with N > 1: one frame per rank (weak scaling, no "
                          "collective) or one frame split by rows (strong scaling, an all-gather)")
+    ap.add_argument("--ref-step-s", type=float, default=0.0,
+                    help="--impl reference: seconds of host work per step (default: the run "
+                         "fits in about three minutes)")
     ap.add_argument("--side", type=int, default=4096, help="stress: image side")
     ap.add_argument("--spp", type=int, default=16, help="stress: samples per pixel")
     args = ap.parse_args()
