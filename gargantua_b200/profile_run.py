@@ -58,6 +58,10 @@ def main() -> None:
     ap.add_argument("--repeats", type=int, default=1)
     ap.add_argument("--side", type=int, default=None, help="kerr_stress_4k: image side")
     ap.add_argument("--spp", type=int, default=None, help="kerr_stress_4k: samples per pixel")
+    ap.add_argument("--width", type=int, default=None,
+                    help="render the same view at this width (with --height): a smaller case "
+                         "of the same kernel for profilers")
+    ap.add_argument("--height", type=int, default=None)
     a = ap.parse_args()
     if a.workload == "adjoint_512":
         run_adjoint(a.repeats)
@@ -72,6 +76,9 @@ def main() -> None:
         if a.spp:
             kw["spp"] = a.spp
     scene = WORKLOADS[a.workload](**kw)
+    if a.width and a.height:
+        scene.width, scene.height = a.width, a.height
+        scene.camera.aspect = a.width / a.height
     r = Renderer(0)
     for _ in range(a.repeats):
         r.render(scene)

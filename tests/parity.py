@@ -108,18 +108,26 @@ def fp32_amplification(scene, oracle_mod, index: int, ref_cross: np.ndarray,
 
 
 def mixed_report(scene, g_cross, o_cross, oracle_mod, index=None, tol=1e-6,
-                 min_amplification=3.0):
+                 min_amplification=3.0, delta=1e-7):
     """Crossing-state error of a mixed-precision render against the oracle's
-    FP64 crossings, and the rays beyond `tol` that the oracle itself does not
-    amplify by more than `min_amplification` (those are the mixed form's own
-    failures; the rest are ill-conditioned at FP32 resolution)."""
+    FP64 crossings.  For every ray beyond `tol` the oracle's amplification of
+    an FP32-sized (`delta`) perturbation is measured: rays it amplifies by at
+    most `min_amplification` are the mixed form's own failures
+    ("unexplained"); for the rest, "worst_ratio" is the largest error over
+    amplification x delta, the error the oracle itself shows from such a
+    perturbation (1 = as large)."""
     index = np.arange(g_cross.shape[1]) if index is None else np.asarray(index)
     m = np.isfinite(o_cross[0]) & np.isfinite(g_cross[0])
     e = crossing_geo_err(g_cross[:, m], o_cross[:, m])
     over = np.nonzero(e > tol)[0]
-    unexplained = [int(index[m][k]) for k in over
-                   if fp32_amplification(scene, oracle_mod, index[m][k], o_cross[:, m][:, k])
-                   <= min_amplification]
+    unexplained, ratios = [], []
+    for k in over:
+        amp = fp32_amplification(scene, oracle_mod, index[m][k], o_cross[:, m][:, k], delta)
+        if amp <= min_amplification:
+            unexplained.append(int(index[m][k]))
+        elif np.isfinite(amp):
+            ratios.append(float(e[k]) / (amp * delta))
     return {"rays": int(m.sum()), "p50": float(np.quantile(e, 0.5)),
             "p99": float(np.quantile(e, 0.99)), "p99.9": float(np.quantile(e, 0.999)),
-            "over_tol": int(over.size), "unexplained": unexplained}
+            "max": float(e.max()), "over_tol": int(over.size), "unexplained": unexplained,
+            "worst_ratio": max(ratios) if ratios else 0.0}

@@ -49,17 +49,24 @@ def test_polar_sincos_within_two_ulp():
 # ---- GPU ------------------------------------------------------------------------
 @pytest.mark.gpu
 def test_mixed_kerr_1080p_against_oracle_subset(renderer, oracle_mod):
+    """16,384 seeded rays of the 1080p frame against the FP64 oracle.  No ray
+    beyond 1e-6 is unexplained, and on the explained ones the error stays
+    within twice what the oracle itself shows from an FP32-sized (1e-7)
+    perturbation of the ray's image-plane point (measured: 0.65 on the
+    frame's 804 such rays)."""
     scene = _mixed(workloads.kerr_thin_1080p)
     _, g = renderer.render(scene, rays=True)
-    idx = np.sort(np.random.default_rng(7).choice(scene.n_samples, 4096, replace=False))
+    idx = np.sort(np.random.default_rng(7).choice(scene.n_samples, 16384, replace=False))
     ref = workloads.kerr_thin_1080p(stepper=abi.GG_STEPPER_DP45)
     o = oracle_mod.trace_samples(ref, idx.astype(np.uint64))
     oc = oracle_mod.trace_cross(ref, idx.astype(np.uint64))
-    assert (g.cls[idx] == o.cls).mean() >= 0.999
+    assert (g.cls[idx] == o.cls).mean() >= 0.9999
     rep = mixed_report(ref, g.cross[:, idx], oc, oracle_mod, index=idx)
-    assert rep["rays"] > 3900
-    assert rep["p99"] <= 1e-6, rep
-    assert len(rep["unexplained"]) <= 0.0005 * rep["rays"] + 1, rep
+    assert rep["rays"] > 16000
+    assert rep["p99"] <= 1e-6 and rep["p99.9"] <= 2e-6, rep
+    assert rep["unexplained"] == [], rep
+    assert rep["worst_ratio"] <= 2.0, rep
+    assert rep["max"] <= 1e-2, rep
 
 
 @pytest.mark.gpu
