@@ -6,11 +6,11 @@
 // that, rounding the state to FP32 every step would cost eps * |x| per step,
 // 1e-5 M at r = 200 after a few hundred steps.  Everything that is small
 // relative to the state runs in FP32: the stage positions and velocities
-// (formed as increments over the state), the seven right-hand sides, and the
-// embedded error estimate, which the Nystrom form builds directly from the
-// stage derivatives (weights c - d), so it carries no cancellation.  The
-// error norm's final reduction and the step-size controller (acceptance test,
-// fifth root, clamps, the step h itself) are FP64.  Attempts that start within
+// (formed as increments over the state) and the seven right-hand sides.  The
+// embedded error estimate -- which the Nystrom form builds directly from the
+// stage derivatives (weights c - d), so it carries no cancellation -- is
+// summed and normed in FP64, and the step-size controller (acceptance test,
+// fifth root, clamps, the step h itself) is FP64.  Attempts that start within
 // 0.5 M of the horizon or of the prograde photon orbit, or near a pole (where
 // Boyer-Lindquist theta turns and is reflected), run in the FP64 pass: the
 // ray is handed over with its state converted to FP64 (gg_mixed.cu).
@@ -26,6 +26,23 @@
 #pragma once
 
 #include "gg_device.cuh"
+
+// Build knobs of the mixed attempt (tuning builds compare them):
+// GG_MIXED_ERR_FP64 (default) forms the embedded error estimate -- its sums
+// over the FP32 stage derivatives and its norm -- in FP64; 0 forms the sums in
+// FP32 and only the norm's reduction in FP64.  Measured on the 1080p Kerr
+// frame: FP64 sums 27.0 ms, FP32 sums 25.4 ms, with the same attempts (416.56
+// M against 416.72 M) and the same crossing-error distribution (p50 1.05e-7,
+// p99 3.9e-7): the estimate's noise comes from the FP32 stage derivatives
+// themselves, which FP64 sums do not remove.  GG_MIXED_STAGE_UNROLL unrolls
+// the seven stages instead of looping over one copy of the right-hand side
+// (26.2 ms: more spills, not kept).
+#ifndef GG_MIXED_ERR_FP64
+#define GG_MIXED_ERR_FP64 1
+#endif
+#ifndef GG_MIXED_STAGE_UNROLL
+#define GG_MIXED_STAGE_UNROLL 0
+#endif
 
 namespace gg {
 
@@ -199,6 +216,25 @@ GG_DEV void error_sums(const MixedSmem& K, float ex[4], float ev[4]) {
   }
 }
 
+// The same sums in FP64 over the FP32 stage derivatives (each product and
+// sum carries the FP64 rounding only), the coefficients in FP64.
+template <int L>
+GG_DEV void error_sums64(const MixedSmem& K, double ex[4], double ev[4]) {
+  if constexpr (L < 7) {
+    constexpr double eb = make_dp_table().Ebar[L], e = make_dp_table().E[L];
+    if constexpr (eb != 0.0 || e != 0.0) {
+      const float4 k4 = K.get(L);
+      const double k[4] = {(double)k4.x, (double)k4.y, (double)k4.z, (double)k4.w};
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        if constexpr (eb != 0.0) ex[i] = fma(eb, k[i], ex[i]);
+        if constexpr (e != 0.0) ev[i] = fma(e, k[i], ev[i]);
+      }
+    }
+    error_sums64<L + 1>(K, ex, ev);
+  }
+}
+
 // Stage S's r, theta and velocity as increments over the state's hi part:
 // x_S = x + h a_S v + h^2 sum Abar k, v_S = v + h sum B k.  Stage 6 is the
 // 5th-order solution: its four position and velocity increments are the
@@ -363,8 +399,9 @@ GG_DEV int attempt_dp45_mixed(const DevParams& P, MixedRegs& S, const MixedSmem&
   const float hh = hf * hf;
   const float r0 = K.comp(kSlotXh, 1), th0 = K.comp(kSlotXh, 2);
   const int s_first = __any_sync(__activemask(), !k1_valid) ? 0 : 1;
-#pragma unroll 1
-  for (int s = s_first; s < 7; ++s) {
+  // One stage: its inputs, the validity test of its position (false: the
+  // attempt ends with h halved), the right-hand side, k_s stored.
+  auto stage = [&](int s) -> bool {
     float pr, pth, pw[4];
     switch (s) {
       case 0:
@@ -380,10 +417,7 @@ GG_DEV int attempt_dp45_mixed(const DevParams& P, MixedRegs& S, const MixedSmem&
       case 5: mixed_stage<5>(r0, th0, S, K, hf, hh, pr, pth, pw); break;
       default: mixed_stage<6>(r0, th0, S, K, hf, hh, pr, pth, pw); break;
     }
-    if (s > 0 && !(isfinite(pr) && isfinite(pth) && pr > 0.0f)) {
-      S.h = S.h * 0.5;
-      return kContinue;
-    }
+    if (s > 0 && !(isfinite(pr) && isfinite(pth) && pr > 0.0f)) return false;
     Geometry32<METRIC> G;
     G.at(P, pr, pth);
     float a[4];
@@ -394,14 +428,63 @@ GG_DEV int attempt_dp45_mixed(const DevParams& P, MixedRegs& S, const MixedSmem&
     // compensated state, so overwriting it would make a ray's result depend
     // on which rays share its warp
     if (s > 0 || !k1_valid) K.set(s, make_float4(a[0], a[1], a[2], a[3]));
+    return true;
+  };
+#if GG_MIXED_STAGE_UNROLL
+  if (s_first == 0) stage(0);
+#pragma unroll
+  for (int s = 1; s < 7; ++s) {
+    if (!stage(s)) {
+      S.h = S.h * 0.5;
+      return kContinue;
+    }
   }
-  float ex[4] = {0.0f, 0.0f, 0.0f, 0.0f}, ev[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-  error_sums<0>(K, ex, ev);
+#else
+#pragma unroll 1
+  for (int s = s_first; s < 7; ++s) {
+    if (!stage(s)) {
+      S.h = S.h * 0.5;
+      return kContinue;
+    }
+  }
+#endif
   const float4 dx4 = K.get(kSlotDx), dv4 = K.get(kSlotDv), xh4 = K.get(kSlotXh);
   const float dx[4] = {dx4.x, dx4.y, dx4.z, dx4.w}, dv[4] = {dv4.x, dv4.y, dv4.z, dv4.w};
   const float xh[4] = {xh4.x, xh4.y, xh4.z, xh4.w};
-  float s2 = 0.0f;
   double err, tol;
+#if GG_MIXED_ERR_FP64
+  // The embedded error estimate in FP64: the sums over the FP32 stage
+  // derivatives (exact in FP64 up to the final rounding), scaled and reduced
+  // in FP64; the per-component scale atol + rtol max(|y|, |y_new|) is a
+  // weight and stays FP32.
+  double ex[4] = {0.0, 0.0, 0.0, 0.0}, ev[4] = {0.0, 0.0, 0.0, 0.0};
+  error_sums64<0>(K, ex, ev);
+  const double hd = (double)hf, hhd = hd * hd;  // both exact
+  double s2 = 0.0;
+  if (P.rtol > 0.0) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const float xs = fmaf(P.rtol_f, fmaxf(fabsf(xh[i]), fabsf(xh[i] + dx[i])), P.atol_f);
+      const float vs = fmaf(P.rtol_f, fmaxf(fabsf(S.vh[i]), fabsf(S.vh[i] + dv[i])), P.atol_f);
+      const double qx = (hhd * ex[i]) * (double)__fdividef(1.0f, xs);
+      const double qv = (hd * ev[i]) * (double)__fdividef(1.0f, vs);
+      s2 = fma(qx, qx, fma(qv, qv, s2));
+    }
+    err = sqrt(s2 * 0.125);
+    tol = 1.0;
+  } else {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const double ax = hhd * ex[i], av = hd * ev[i];
+      s2 = fma(ax, ax, fma(av, av, s2));
+    }
+    err = sqrt(s2);
+    tol = P.tolerance;
+  }
+#else
+  float ex[4] = {0.0f, 0.0f, 0.0f, 0.0f}, ev[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+  error_sums<0>(K, ex, ev);
+  float s2 = 0.0f;
   if (P.rtol > 0.0) {
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
@@ -422,6 +505,7 @@ GG_DEV int attempt_dp45_mixed(const DevParams& P, MixedRegs& S, const MixedSmem&
     err = sqrt((double)s2);
     tol = P.tolerance;
   }
+#endif
   if (err < tol || S.h <= P.min_step) {
     accepted = true;
     if (err > 0.0) {
