@@ -242,6 +242,51 @@ def time_form(r, scene, steps, warmup, world, flush, with_clocks, device_index, 
     return {"ms": ms, "total_ms": total_ms, "stats": st, "clocks": clocks}
 
 
+def turned_camera(scene, du: float, dv: float):
+    """`scene` with its camera turned so that every pixel's direction moves
+    by about du (horizontal) and dv (vertical) image-plane units: look_at
+    rotated about the camera's up axis by du tan(fov/2) aspect and towards
+    its up vector by dv tan(fov/2)."""
+    import copy
+    import math
+
+    import numpy as np
+    cam = scene.camera
+    f = np.array(cam.look_at, float)
+    f /= np.linalg.norm(f)
+    up = np.array(cam.up, float)
+    right = np.cross(f, up)
+    right /= np.linalg.norm(right)
+    up2 = np.cross(right, f)
+    t = math.tan(0.5 * cam.fov_y_radians)
+    a_u, a_v = du * t * cam.aspect, dv * t
+    g = math.cos(a_u) * f + math.sin(a_u) * right
+    g = math.cos(a_v) * g + math.sin(a_v) * up2
+    s = copy.copy(scene)
+    c = copy.copy(cam)
+    c.look_at = tuple(float(x) for x in g)
+    s.camera = c
+    return s
+
+
+def fp64_amplification(r, scene64, g64, mask, delta: float = 1e-7):
+    """Per ray, how much the FP64 kernel amplifies an image-plane
+    perturbation of `delta`: the crossing-state change (crossing_geo_err)
+    under a camera turned by delta in u, and in v, over delta; the larger of
+    the two (inf where the turned ray does not cross)."""
+    import numpy as np
+
+    from gargantua_b200.accuracy import crossing_geo_err
+    amp = np.zeros(g64.cls.shape[0])
+    for du, dv in ((delta, 0.0), (0.0, delta)):
+        _, gt = r.render(turned_camera(scene64, du, dv), rays=True)
+        ok = mask & np.isfinite(gt.cross[0])
+        e = np.full(amp.shape, np.inf)
+        e[ok] = crossing_geo_err(gt.cross[:, ok], g64.cross[:, ok]) / delta
+        amp = np.maximum(amp, e)
+    return amp
+
+
 def time_e2e(r, scene, steps, warmup, world):
     import numpy as np
     import torch
@@ -318,14 +363,8 @@ def run_ours(args) -> None:
     from gargantua_b200.accuracy import crossing_geo_err
     from gargantua_b200.curved import Renderer
 
-    rank, world, local = dist_env()
-    torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device(f"cuda:{local}"))
+    rank, _, local = dist_env()
+    world = init_dist(local, 600)
     steps, warmup = args.steps, max(3, args.warmup)
     r = Renderer(local)
     flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device="cuda")
@@ -390,11 +429,25 @@ def run_ours(args) -> None:
     both = np.isfinite(g_mx.cross[0]) & np.isfinite(g_64.cross[0])
     err = crossing_geo_err(g_mx.cross[:, both], g_64.cross[:, both])
     eq = np.quantile(err, [0.5, 0.9, 0.99, 0.999, 0.9999, 1.0]).tolist()
+    # rays beyond 1e-6: is each one ill-conditioned at FP32 resolution?  The
+    # FP64 kernel re-renders the frame with the camera turned by an
+    # image-plane step of 1e-7 in u and in v; a ray whose crossing state then
+    # moves by more than 3 x 1e-7 (amplification > 3) cannot hold 1e-6 in any
+    # FP32 representation of its state
+    amp = fp64_amplification(r, forms["fp64_dp45"]["scene"], g_64, both)
+    over = err > 1e-6
+    explained = over & (amp[both] > 3.0)
     endpoint = {"reference": "FP64 kernel, same stepper, same samples", "rays": int(both.sum()),
                 "measure": "max(|dx_cart|/r, |dv_cart|/|v_cart|, |dt|/t, |dv^t|/v^t) at the "
                            "escape-sphere or disk-plane crossing",
                 "p50": eq[0], "p90": eq[1], "p99": eq[2], "p99.9": eq[3], "p99.99": eq[4],
                 "max": eq[5], "frac_le_1e-6": float((err <= 1e-6).mean()),
+                "over_1e-6": int(over.sum()), "over_1e-6_explained": int(explained.sum()),
+                "over_1e-6_unexplained": int((over & ~explained).sum()),
+                "frac_le_1e-6_or_explained": float(((err <= 1e-6) | explained).mean()),
+                "explained_by": "FP64 kernel re-rendered with the camera turned by a 1e-7 "
+                                "image-plane step in u and in v: crossing-state change over "
+                                "1e-7 above 3",
                 "class_agreement": float((g_mx.cls == g_64.cls).mean())}
 
     # end to end through gg_render (host pinned output)
@@ -448,42 +501,107 @@ def run_ours(args) -> None:
     line["endpoint_error"] = endpoint
     line["mixed_over_fp64"] = H["geodesics_per_s"] / forms["fp64"]["geodesics_per_s"]
     line["mixed_over_fp64_dp45"] = H["geodesics_per_s"] / forms["fp64_dp45"]["geodesics_per_s"]
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    cpu = rank == 0 and world == 1 and not args.no_cpu_baseline
+    if cpu:
         line["cpu_baseline"] = cpu_baseline(forms["fp64"]["scene"])
+    if not args.no_configs:
+        # the other configurations, each with its own device time, clocks,
+        # attempts, roofline fraction and CPU baseline (short runs)
+        peaks = {"fp64": fp64_peak, "fp32": fp32_peak}
+        k = min(steps, 10)
+        line["c1_schwarzschild_256"] = measure_c1(r, steps, warmup, world, local, flush, peaks,
+                                                  cpu)
+        line["c3_batch_2048"] = measure_batch(r, 2048, 2, 2, world, rank, local, peaks, cpu,
+                                              False, 8.0)
+        line["c4_adjoint_512"] = measure_adjoint(r, k, 3, world, rank, local, flush, peaks, cpu,
+                                                 8.0)
+        line["c5_stress_4096x4096x16"] = measure_stress(r, 4096, 16, world, rank, local, peaks,
+                                                        cpu, 8.0)
     r.close()
-    if world > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    close_dist(world)
     if rank == 0:
         print(json.dumps(line), flush=True)
 
 
-# ---- stress configuration ------------------------------------------------------------
-def run_stress(args) -> None:
-    """Near-extremal Kerr a = 0.998, side x side pixels x spp seeded jittered
-    samples (default 4096 x 4096 x 16), camera r = 15 M at 85 deg, disk
-    r_ISCO-25 M, 50,000 step() calls per ray: one frame per form (plain FP64,
-    FP64 full Dormand-Prince, mixed), timed with CUDA events after a warm-up
-    frame of 256 x 256 x 1, and the per-ray attempt distribution.  Per-ray
-    outputs stay on the device (attempts and class only).  With N ranks
-    (torchrun) each traces its interleaved rows of the frame (shard.shard_scene;
-    jitter is keyed by the global sample, so the frame is the same); times
-    are the max over ranks, counts and histograms sums."""
+# ---- shared by the configuration measurements ----------------------------------------
+def init_dist(local: int, timeout_s: int = 300):
+    """Process group of a torchrun launch (NCCL), or None on one GPU."""
     import torch
-
-    from gargantua_b200 import abi, shard, workloads
-    from gargantua_b200.curved import Renderer
-
-    rank, world, local = dist_env()
+    rank, world, _ = dist_env()
     torch.cuda.set_device(local)
     if world > 1:
         import datetime
 
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=timeout_s),
                                 device_id=torch.device(f"cuda:{local}"))
-    r = Renderer(local)
-    side, spp = args.side, args.spp
+    return world
+
+
+def close_dist(world: int) -> None:
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def roofline_entry(attempts: int, flops_per_attempt: int, seconds: float, peak: float,
+                   bound: str, kernel: str) -> dict:
+    """Counted FLOPs of `attempts` RK45 attempts over `seconds`, against the
+    FMA peak measured in this run."""
+    achieved = attempts * flops_per_attempt / seconds
+    return {"bound": bound, "achieved": achieved / 1e12, "peak": peak / 1e12,
+            "unit": "TFLOP/s", "frac": achieved / peak, "kernel": kernel,
+            "flops_per_attempt": flops_per_attempt,
+            "peak_source": "measured in this run by gg_measure_fma_peak (FMA chains)"}
+
+
+# ---- the 256 x 256 Schwarzschild frame (plain FP64) --------------------------------------
+def measure_c1(r, steps: int, warmup: int, world: int, local: int, flush, peaks: dict,
+               cpu: bool) -> dict:
+    """The plain method on the CPU-runnable frame: Schwarzschild M = 1, 256 x 256,
+    camera r = 30 M at 80 deg, thin disk 6-20 M, rtol 1e-8 / atol 1e-10, 10,000
+    step() calls, the FP64 drop-in (the reference's step).  Each rank renders
+    its own copy of the frame (weak scaling); the CPU baseline traces the whole
+    frame through the oracle."""
+    from gargantua_b200 import abi, flops, workloads
+    scene = workloads.schwarzschild_thin_256()
+    res = time_form(r, scene, steps, warmup, world, flush, True, local, False)
+    st = res["stats"]
+    sec = res["total_ms"] * 1e-3 / steps
+    attempts = sum_over_ranks(int(st.attempts), world)
+    out = {"workload": "schwarzschild_256x256_thin_disk", "form": "fp64 (reference step)",
+           "samples_per_step": scene.n_samples * world,
+           "ms_per_step": res["total_ms"] / steps,
+           "geodesics_per_s": scene.n_samples * world / sec,
+           "attempts_per_frame": attempts, "accepted_per_frame":
+               sum_over_ranks(int(st.accepted), world),
+           "class_count": [int(x) for x in st.class_count], "clocks": res["clocks"],
+           "roofline": roofline_entry(int(st.attempts), flops.attempt_flops(
+               "schwarzschild", scene.integrator_c().rtol, abi.GG_STEPPER_REFERENCE),
+               statistics.mean(res["ms"]) * 1e-3, peaks["fp64"], "fp64",
+               "trace_fp64_kernel<Schwarzschild, ThinDisk>")}
+    if cpu:
+        out["cpu_baseline"] = cpu_baseline(scene, 30.0, "the 256x256 frame")
+    return out
+
+
+# ---- stress configuration ------------------------------------------------------------
+def measure_stress(r, side: int, spp: int, world: int, rank: int, local: int, peaks: dict,
+                   cpu: bool, cpu_target_s: float = 10.0) -> dict:
+    """Near-extremal Kerr a = 0.998, side x side pixels x spp seeded jittered
+    samples (4096 x 4096 x 16 by default), camera r = 15 M at 85 deg, disk
+    r_ISCO-25 M, 50,000 step() calls per ray: one frame per form (plain FP64,
+    FP64 full Dormand-Prince, mixed), timed with CUDA events after a warm-up
+    frame of 256 x 256 x 1, with clocks sampled during the frames, and the
+    per-ray attempt distribution.  Per-ray outputs stay on the device
+    (attempts and class only).  With N ranks each traces its interleaved rows
+    of the frame (shard.shard_scene; jitter is keyed by the global sample, so
+    the frame is the same); times are the max over ranks, counts and
+    histograms sums."""
+    import torch
+
+    from gargantua_b200 import abi, flops, shard, workloads
+
     n = side * side * spp
     rows = shard.rows_of(side, rank, world)
     n_mine = rows * side * spp
@@ -514,11 +632,13 @@ def run_stress(args) -> None:
         rays.cls = C.cast(C.c_void_p(cls.data_ptr()), C.POINTER(C.c_int32))
         stream.synchronize()
         barrier(world)
+        clk = ClockSampler(local)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         r.render_device(scene, img.data_ptr(), rays, r.stream)
         e1.record(stream)
         stream.synchronize()
+        clocks = clk.stop()
         ms = max_over_ranks(e0.elapsed_time(e1), world)
         st = r.stats()
         a = att.to(torch.int64)
@@ -527,11 +647,20 @@ def run_stress(args) -> None:
         sums = reduce_sum([int(st.attempts), int(st.accepted), int(st.fp64_rays),
                            int(st.fp64_attempts)] + [int(x) for x in st.class_count] + hist)
         nc = len(st.class_count)
+        mixed = form == "mixed"
+        fpa = flops.attempt_flops("kerr", 1e-8, abi.GG_STEPPER_REFERENCE if form == "fp64"
+                                  else abi.GG_STEPPER_DP45)
         entry = {"ms": ms, "geodesics_per_s": n / (ms * 1e-3),
                  "attempts": sums[0], "accepted": sums[1],
                  "attempts_per_s": sums[0] / (ms * 1e-3),
                  "class_count": sums[4:4 + nc],
                  "fp64_band_rays": sums[2], "fp64_band_attempts": sums[3],
+                 "clocks": clocks,
+                 "roofline": roofline_entry(sums[0] // world, fpa, ms * 1e-3,
+                                            peaks["fp32" if mixed else "fp64"],
+                                            "fp32" if mixed else "fp64",
+                                            "trace_mixed_kernel + FP64 band passes" if mixed
+                                            else "trace_fp64_kernel<Kerr, ThinDisk>"),
                  "attempts_histogram": {"bin_lower_edges": edges[:-1] + [edges[-1]],
                                         "counts": sums[4 + nc:]}}
         if world == 1:
@@ -555,42 +684,45 @@ def run_stress(args) -> None:
             "mixed_over_fp64_dp45": (forms["mixed"]["geodesics_per_s"]
                                      / forms["fp64_dp45"]["geodesics_per_s"]),
             "class_agreement_mixed_vs_fp64_dp45": agree / n}
+    if cpu and rank == 0 and world == 1:
+        line["cpu_baseline"] = cpu_baseline(workloads.kerr_stress_4k(side=side, spp=spp),
+                                            cpu_target_s, f"the {side}x{side}x{spp} spp frame")
+    return line
+
+
+def run_stress(args) -> None:
+    """--workload stress: the stress configuration as its own JSON line."""
+    from gargantua_b200.curved import Renderer
+    rank, _, local = dist_env()
+    world = init_dist(local, 600)
+    r = Renderer(local)
+    peaks = {"fp64": r.fma_peak(fp64=True), "fp32": r.fma_peak(fp64=False)}
+    line = measure_stress(r, args.side, args.spp, world, rank, local, peaks,
+                          not args.no_cpu_baseline)
     r.close()
-    if world > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    close_dist(world)
     if rank == 0:
-        if world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(workloads.kerr_stress_4k(side=side, spp=spp), 10.0,
-                                                f"the {side}x{side}x{spp} spp frame")
         print(json.dumps(line), flush=True)
 
 
 # ---- batched scenes --------------------------------------------------------------------
-def run_batch(args) -> None:
-    """2,048 independent Kerr scenes of uneven size (workloads.batch_scenes:
+def measure_batch(r, n_scenes: int, steps: int, warmup: int, world: int, rank: int,
+                  local: int, peaks: dict, cpu: bool, one_launch_each: bool,
+                  cpu_target_s: float = 10.0) -> dict:
+    """n_scenes independent Kerr scenes of uneven size (workloads.batch_scenes:
     spin, camera distance and inclination, image side 64..512, disk outer
     radius drawn per scene, seed 0), mixed precision, in one persistent
     launch replayed from a CUDA graph, after autotuning the kernel variant on
-    every 8th scene.  With N ranks (torchrun) each renders the scenes
+    every 8th scene.  With N ranks each renders the scenes
     shard.partition_scenes gives it (cost-balanced, no data-path
-    collective); a step is timed as the max over ranks.  Beside it, at N=1:
-    the same scenes rendered one launch each."""
+    collective); a step is timed as the max over ranks.  With
+    one_launch_each (N = 1) the same scenes are also rendered one launch
+    each."""
     import torch
 
-    from gargantua_b200 import shard, workloads
-    from gargantua_b200.curved import Renderer
+    from gargantua_b200 import abi, flops, shard, workloads
 
-    rank, world, local = dist_env()
-    torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device(f"cuda:{local}"))
-    r = Renderer(local)
-    scenes = workloads.batch_scenes(args.scenes, seed=0)
+    scenes = workloads.batch_scenes(n_scenes, seed=0)
     parts = shard.partition_scenes(scenes, world)
     mine = [scenes[k] for k in parts[rank]]
     n = sum(sc.n_samples for sc in scenes)
@@ -600,11 +732,12 @@ def run_batch(args) -> None:
     t0 = time.perf_counter()
     variant, tune_ms = r.batch_autotune(mine[::8])
     tune_s = time.perf_counter() - t0
-    steps, warmup = max(1, args.steps // 3), max(3, args.warmup)
     for _ in range(warmup):
         r.render_batch_device(mine, out.data_ptr(), r.stream)
     stream.synchronize()
     ms = []
+    barrier(world)
+    clk = ClockSampler(local)
     for _ in range(steps):
         barrier(world)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -613,6 +746,7 @@ def run_batch(args) -> None:
         e1.record(stream)
         stream.synchronize()
         ms.append(max_over_ranks(e0.elapsed_time(e1), world))
+    clocks = clk.stop()
     st = r.stats()
     attempts = sum_over_ranks(int(st.attempts), world)
     band_rays = sum_over_ranks(int(st.fp64_rays), world)
@@ -629,14 +763,20 @@ def run_batch(args) -> None:
                        "parallelism": f"scenes over {world} rank(s), cost-balanced "
                                       "(shard.partition_scenes)",
                        "l2": "outputs (3 B per sample, 625 MB) larger than L2"},
-            "value": n / (best * 1e-3), "ms_per_batch": ms,
+            "value": n / (best * 1e-3), "ms_per_batch": ms, "clocks": clocks,
             "rays": rays, "attempts": attempts, "attempts_per_s": attempts / (best * 1e-3),
             "fp64_band_rays": band_rays, "fp64_band_attempts": band_att,
+            "roofline": roofline_entry(int(st.attempts), flops.attempt_flops(
+                "kerr", 1e-8, abi.GG_STEPPER_DP45), best * 1e-3, peaks["fp32"], "fp32",
+                "trace_mixed_kernel<Kerr, ThinDisk, BATCH> + FP64 band passes"),
             "autotune": {"variant": variant, "variant_ms_on_every_8th_scene": tune_ms,
-                         "variants": "0..5 = (period, CTAs/SM) (16,8) (8,8) (4,8) (16,7) (32,7) (32,8)",
+                         "variants": abi.batch_variant_names(),
                          "wall_s": tune_s}}
     if world == 1:
         line["class_count"] = [int(x) for x in st.class_count]
+    else:
+        line["samples_per_rank"] = [sum(scenes[k].n_samples for k in p) for p in parts]
+    if one_launch_each and world == 1:
         # the same scenes, one launch each (single-scene entry point, same kernel family)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         off = 0
@@ -653,15 +793,23 @@ def run_batch(args) -> None:
         line["one_launch_per_scene"] = {"ms": single_ms,
                                         "geodesics_per_s": n / (single_ms * 1e-3)}
         line["batch_over_one_launch_per_scene"] = single_ms / best
-    else:
-        line["samples_per_rank"] = [sum(scenes[k].n_samples for k in p) for p in parts]
+    if cpu and rank == 0 and world == 1:
+        line["cpu_baseline"] = cpu_baseline_batch(scenes, cpu_target_s)
+    return line
+
+
+def run_batch(args) -> None:
+    """--workload batch: the batching configuration as its own JSON line."""
+    from gargantua_b200.curved import Renderer
+    rank, _, local = dist_env()
+    world = init_dist(local)
+    r = Renderer(local)
+    peaks = {"fp64": r.fma_peak(fp64=True), "fp32": r.fma_peak(fp64=False)}
+    line = measure_batch(r, args.scenes, max(1, args.steps // 3), max(3, args.warmup), world,
+                         rank, local, peaks, not args.no_cpu_baseline, True)
     r.close()
-    if world > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    close_dist(world)
     if rank == 0:
-        if world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline_batch(scenes)
         print(json.dumps(line), flush=True)
 
 
@@ -703,32 +851,23 @@ def cpu_baseline_fd(dscene, p, target_s: float = 20.0) -> dict:
                       "host threads, extrapolated to the whole image"}
 
 
-def run_adjoint(args) -> None:
+def measure_adjoint(r, steps: int, warmup: int, world: int, rank: int, local: int, flush,
+                    peaks: dict, cpu: bool, cpu_target_s: float = 20.0) -> dict:
     """The differentiation configuration: Kerr 512 x 512, L2 loss of the image
     against a target rendered at (a = 0.7, inclination 60 deg, r_cam = 40 M,
     r_in = r_ISCO, q = 3), parameters perturbed by N(0, 5 %) (seed 0).  A step
     is one gradient: the forward with checkpoints every 32 accepted steps
     (gg_forward_ckpt), dL/d(image), and the adjoint (gg_backward) to the five
-    parameters.  With N ranks (torchrun) each differentiates its interleaved
-    rows and the five sums are all-reduced (NCCL) inside the step, the one
+    parameters.  With N ranks each differentiates its interleaved rows and
+    the five sums are all-reduced (NCCL) inside the step, the one
     collective; the step time is the max over ranks.  Beside it at N=1: the
-    central differences the adjoint replaces (ten forwards at p +- 1e-6 p_i) on
-    the GPU, and through the oracle on the host cores (cpu_baseline)."""
+    central differences the adjoint replaces (ten forwards at p +- 1e-6 p_i)
+    on the GPU, and through the oracle on the host cores (cpu_baseline)."""
     import numpy as np
     import torch
 
     from gargantua_b200 import abi, diff, flops
-    from gargantua_b200.curved import Renderer
 
-    rank, world, local = dist_env()
-    torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device(f"cuda:{local}"))
-    r = Renderer(local)
     whole = diff.DiffScene()
     dscene = whole.shard(rank, world)
     dr = diff.DiffRenderer(dscene, r)
@@ -737,7 +876,6 @@ def run_adjoint(args) -> None:
     target = torch.empty(dr.n_values, dtype=torch.float64, device="cuda")
     img = torch.empty_like(target)
     dl = torch.empty_like(target)
-    flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device="cuda")
     dr.forward_into(diff.target_params(), target.data_ptr(), r.stream)
     stream.synchronize()
 
@@ -758,7 +896,6 @@ def run_adjoint(args) -> None:
                 ev[3].record(stream)
         return g
 
-    steps, warmup = args.steps, max(3, args.warmup)
     for _ in range(warmup):
         g = gradient()
     stream.synchronize()
@@ -808,9 +945,6 @@ def run_adjoint(args) -> None:
     r.render(dscene.scene_at(p))
     attempts = sum_over_ranks(int(r.stats().attempts), world)
     fpa = flops.attempt_flops("kerr", whole.integrator.rtol, abi.GG_STEPPER_DP45)
-    fp64_peak = r.fma_peak(fp64=True)
-    achieved = attempts / world * fpa / (fwd_ms * 1e-3)
-
     line = {"metric": "Kerr 512^2 adjoint: gradients/s (forward + backward, 5 parameters)",
             "value": steps / (total_ms * 1e-3), "unit": "gradients/s", "n_gpus": world,
             "steps": steps, "warmup": warmup, "ms_per_step": ms, "higher_is_better": True,
@@ -836,12 +970,11 @@ def run_adjoint(args) -> None:
                     "d2h_bytes_per_step": 5 * 8 + 8,
                     "via": "diff.kerr_image (torch.autograd.Function) + loss.backward()"},
             "gpu_launches": 2 * steps,
-            "roofline": {"bound": "fp64", "achieved": achieved / 1e12, "peak": fp64_peak / 1e12,
-                         "unit": "TFLOP/s", "frac": achieved / fp64_peak, "traffic": None,
-                         "kernel": "trace_fp64_kernel<Kerr, ThinDisk, DP45, camera, CKPT> (the "
-                                   "forward; the backward's dual-number work is not counted)",
-                         "flops_per_attempt": fpa, "forward_attempts": attempts,
-                         "peak_source": "measured in this run by gg_measure_fma_peak (FMA chains)"}}
+            "roofline": dict(roofline_entry(attempts // world, fpa, fwd_ms * 1e-3, peaks["fp64"],
+                                            "fp64", "trace_fp64_kernel<Kerr, ThinDisk, DP45, "
+                                            "camera, CKPT> (the forward; the backward's "
+                                            "dual-number work is not counted)"),
+                             traffic=None, forward_attempts=attempts)}
     if world == 1:
         # central differences on the GPU: ten forwards and their losses
         fd = torch.empty_like(target)
@@ -860,13 +993,26 @@ def run_adjoint(args) -> None:
         fd_ms = e0.elapsed_time(e1)
         line["central_differences_gpu"] = {"ms": fd_ms, "adjoint_speedup": fd_ms / ms}
         line["e2e"]["loss"] = e2e_loss
+    if cpu and rank == 0 and world == 1:
+        line["cpu_baseline"] = cpu_baseline_fd(whole, p, cpu_target_s)
+    return line
+
+
+def run_adjoint(args) -> None:
+    """--workload adjoint: the differentiation configuration as its own JSON line."""
+    import torch
+
+    from gargantua_b200.curved import Renderer
+    rank, _, local = dist_env()
+    world = init_dist(local)
+    r = Renderer(local)
+    flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    peaks = {"fp64": r.fma_peak(fp64=True), "fp32": r.fma_peak(fp64=False)}
+    line = measure_adjoint(r, args.steps, max(3, args.warmup), world, rank, local, flush, peaks,
+                           not args.no_cpu_baseline)
     r.close()
-    if world > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    close_dist(world)
     if rank == 0:
-        if world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline_fd(whole, p)
         print(json.dumps(line), flush=True)
 
 
@@ -1058,6 +1204,9 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="kerr1080p: skip the other configurations' entries (256^2 "
+                         "Schwarzschild, 2,048-scene batch, 512^2 adjoint, 4096^2 x 16 stress)")
     ap.add_argument("--workload", choices=["kerr1080p", "stress", "batch", "adjoint", "features"],
                     default="kerr1080p",
                     help="stress: the a=0.998 4096^2 x 16 spp configuration (one frame per "

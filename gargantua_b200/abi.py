@@ -36,6 +36,13 @@ GG_PREC_MIXED = 1
 GG_STEPPER_REFERENCE = 0
 GG_STEPPER_DP45 = 1
 GG_BATCH_VARIANTS = 6
+# (refill period, CTAs per SM) of each batch kernel variant, by index
+BATCH_VARIANTS = ((16, 8), (8, 8), (4, 8), (16, 7), (32, 7), (32, 8))
+
+
+def batch_variant_names() -> list[str]:
+    """The batch kernel variants gg_batch_autotune chooses from, by index."""
+    return [f"period {p}, {m} CTAs/SM" for p, m in BATCH_VARIANTS]
 GG_SKY_PROCEDURAL = 0
 GG_SKY_CHECKER = 1
 GG_SKY_HDRI = 2

@@ -45,3 +45,19 @@ def test_oracle_traces_each_feature_case(name):
     cls = np.asarray(ra.cls)
     assert np.all((cls >= 0) & (cls <= 5))
     assert np.all(np.asarray(ra.attempts) > 0)
+
+
+def test_turned_camera_moves_the_view_by_the_image_plane_step():
+    # the bench's amplification probe turns the camera so that each pixel
+    # moves by about one image-plane step of du (or dv)
+    import math
+    sc = workloads.kerr_thin_1080p()
+    f0 = np.array(sc.camera.look_at) / np.linalg.norm(sc.camera.look_at)
+    t = math.tan(0.5 * sc.camera.fov_y_radians)
+    for du, dv, want in ((1e-3, 0.0, 1e-3 * t * sc.camera.aspect), (0.0, 1e-3, 1e-3 * t)):
+        s2 = bench.turned_camera(sc, du, dv)
+        f1 = np.array(s2.camera.look_at)
+        assert abs(np.linalg.norm(f1) - 1.0) < 1e-12
+        assert abs(math.acos(min(1.0, float(f0 @ f1))) - want) < 1e-9
+        assert s2.camera.position == sc.camera.position and s2.camera.up == sc.camera.up
+    assert sc.camera.look_at == workloads.kerr_thin_1080p().camera.look_at  # not modified

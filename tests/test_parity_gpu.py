@@ -21,11 +21,13 @@ Parity bar (plain FP64 form):
 """
 from __future__ import annotations
 
+import ctypes as C
+
 import numpy as np
 import pytest
 
 from gargantua_b200 import abi, workloads
-from gargantua_b200.curved import CheckerSky, RenderOptions, Scene, ThinDisk
+from gargantua_b200.curved import CheckerSky, RayOutputs, RenderOptions, Scene, ThinDisk
 from gargantua_b200.gr_core import Kerr, Schwarzschild
 from parity import compare
 
@@ -115,6 +117,42 @@ def test_jittered_samples_match_oracle(renderer, oracle_mod):
     # endpoints diverge chaotically; every other sample must meet 1e-9
     compare(scene, g, o, oracle_mod, max_excluded=0.01)
     assert (np.abs(img.astype(int) - oimg.astype(int)) <= 1).all(axis=2).mean() > 0.99
+
+
+def test_stress_frame_seeded_subset(renderer, oracle_mod):
+    """The full stress frame -- Kerr a = 0.998, 4096 x 4096 x 16 seeded
+    jittered samples, camera r = 15 M at 85 deg, 50,000 step() calls -- in
+    FP64 on the GPU, and 4,096 seeded samples of it against the oracle.  The
+    frame's outputs stay on the device (class, x, v, attempts: 19 GB); only
+    the subset comes back."""
+    import torch
+    scene = workloads.kerr_stress_4k()
+    n = scene.n_samples
+    assert n == 4096 * 4096 * 16 and scene.options.max_steps == 50000
+    cls = torch.empty(n, dtype=torch.int32, device="cuda")
+    att = torch.empty(n, dtype=torch.int32, device="cuda")
+    x = torch.empty(4 * n, dtype=torch.float64, device="cuda")
+    v = torch.empty(4 * n, dtype=torch.float64, device="cuda")
+    rays = abi.gg_ray_out_t()
+    for name, t, ct in (("cls", cls, C.c_int32), ("attempts", att, C.c_uint32),
+                        ("x", x, C.c_double), ("v", v, C.c_double)):
+        setattr(rays, name, C.cast(C.c_void_p(t.data_ptr()), C.POINTER(ct)))
+    stream = torch.cuda.current_stream(0)
+    renderer.render_device(scene, 0, rays, stream.cuda_stream)
+    stream.synchronize()
+    st = renderer.stats()
+    assert st.rays == n
+    idx = np.sort(np.random.default_rng(5).choice(n, 4096, replace=False))
+    ti = torch.from_numpy(idx.astype(np.int64)).cuda()
+    g = RayOutputs(len(idx))
+    g.cls = cls[ti].cpu().numpy()
+    g.attempts = att[ti].cpu().numpy().view(np.uint32)
+    g.x = x.view(4, n)[:, ti].cpu().numpy()
+    g.v = v.view(4, n)[:, ti].cpu().numpy()
+    del cls, att, x, v
+    o = oracle_mod.trace_samples(scene, idx.astype(np.uint64))
+    assert o.attempts.max() > 200  # the subset reaches the photon-ring grazers
+    compare(scene, g, o, oracle_mod, idx=idx, max_excluded=0.01)
 
 
 def test_device_pointer_render_matches_host(renderer):
