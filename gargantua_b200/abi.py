@@ -35,14 +35,21 @@ GG_PREC_FP64 = 0
 GG_PREC_MIXED = 1
 GG_STEPPER_REFERENCE = 0
 GG_STEPPER_DP45 = 1
-GG_BATCH_VARIANTS = 6
-# (refill period, CTAs per SM) of each batch kernel variant, by index
-BATCH_VARIANTS = ((16, 8), (8, 8), (4, 8), (16, 7), (32, 7), (32, 8))
+GG_BATCH_VARIANTS = 12
+
+
+def batch_variant(v: int) -> tuple[int, int, int, int]:
+    """(refill period, CTAs per SM, threads per CTA, samples per queue claim)
+    of batch kernel variant v (gg_batch_variant_info)."""
+    out = (C.c_int32 * 4)()
+    check(load().gg_batch_variant_info(int(v), out), "gg_batch_variant_info")
+    return tuple(out)
 
 
 def batch_variant_names() -> list[str]:
     """The batch kernel variants gg_batch_autotune chooses from, by index."""
-    return [f"period {p}, {m} CTAs/SM" for p, m in BATCH_VARIANTS]
+    return ["period {}, {} CTAs/SM, {} threads, chunk {}".format(*batch_variant(v))
+            for v in range(GG_BATCH_VARIANTS)]
 GG_SKY_PROCEDURAL = 0
 GG_SKY_CHECKER = 1
 GG_SKY_HDRI = 2
@@ -171,6 +178,7 @@ _SIGNATURES = {
     "gg_batch_autotune": (C.c_int, [C.c_void_p, P(gg_scene_t), C.c_uint32, P(gg_integrator_t),
                                     P(gg_render_opts_t), P(C.c_int), P(C.c_double)]),
     "gg_batch_set_variant": (C.c_int, [C.c_void_p, C.c_int]),
+    "gg_batch_variant_info": (C.c_int, [C.c_int, C.c_void_p]),
     "gg_set_hdri": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_float]),
     "gg_set_scene": (C.c_int, [C.c_void_p, P(gg_prim_t), C.c_uint32]),
     "gg_scene_validate": (C.c_int, [P(gg_prim_t), C.c_uint32, P(C.c_uint32), P(C.c_uint32)]),

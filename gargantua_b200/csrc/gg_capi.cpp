@@ -1115,6 +1115,16 @@ GG_API int gg_scene_validate(const gg_prim_t* prims, uint32_t n, uint32_t* n_nod
   return st;
 }
 
+GG_API int gg_batch_variant_info(int v, int32_t out[4]) {
+  if (!out || v < 0 || v >= GG_BATCH_VARIANTS) return GG_ERR_INVALID_ARG;
+  const gg::BatchVariant& b = gg::kBatchVariantTable[v];
+  out[0] = b.period;
+  out[1] = b.ctas_per_sm;
+  out[2] = b.block;
+  out[3] = b.chunk;
+  return GG_OK;
+}
+
 GG_API int gg_batch_set_variant(gg_ctx* c, int variant) {
   if (!c || variant < 0 || variant >= GG_BATCH_VARIANTS) return GG_ERR_INVALID_ARG;
   Lock lock(c);

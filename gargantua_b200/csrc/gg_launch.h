@@ -68,7 +68,16 @@ cudaError_t launch_trace(const DevParams& P, const DevOutputs& O, DevControl* ct
 // and a last FP64 pass without hand-back.
 // A batched render (batch != nullptr) runs one of kBatchVariants kernel
 // variants (compaction period x register budget), chosen by `variant`.
-constexpr int kBatchVariants = 6;
+struct BatchVariant {
+  int period, ctas_per_sm, block, chunk;
+};
+// Refill period, CTAs per SM (the register budget: 65536 / (block * CTAs)
+// per thread), threads per CTA and samples a warp claims per queue access.
+constexpr BatchVariant kBatchVariantTable[] = {
+    {16, 8, 128, 32}, {8, 8, 128, 32},  {4, 8, 128, 32},  {16, 7, 128, 32},
+    {32, 7, 128, 32}, {32, 8, 128, 32}, {32, 16, 64, 32}, {16, 16, 64, 32},
+    {32, 4, 256, 32}, {16, 4, 256, 32}, {32, 8, 128, 16}, {32, 8, 128, 64}};
+constexpr int kBatchVariants = (int)(sizeof(kBatchVariantTable) / sizeof(kBatchVariantTable[0]));
 cudaError_t mixed_occupancy(const DevParams& P, int* blocks_per_sm,
                             const BatchTable* batch = nullptr, int variant = 0,
                             bool returned = false);

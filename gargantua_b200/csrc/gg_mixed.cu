@@ -22,6 +22,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <utility>
 
 #include "../../include/gargantua_gpu.h"
 #include "gg_device.cuh"
@@ -36,7 +37,8 @@ namespace {
 // Writes the ray to the FP64 pass's queue (out of line: once per handed-off
 // ray).  The state is the one the next attempt starts from.  The register
 // part of the ray comes by value, so the stepping loop keeps it in registers.
-__device__ __noinline__ void hand_off(const DevOutputs& O, DevControl* ctl, MixedSmem K,
+template <class KS>
+__device__ __noinline__ void hand_off(const DevOutputs& O, DevControl* ctl, KS K,
                                       MixedRegs S, uint32_t n_att, uint32_t n_acc,
                                       uint32_t scene) {
   const unsigned long long slot = atomicAdd(&ctl->queued, 1ull);
@@ -71,7 +73,8 @@ GG_DEV uint32_t find_scene(const BatchTable& B, uint64_t g) {
 
 // Writes a finished ray's outcome (its state converted to FP64) and counts it
 // in the block's statistics.  Out of line, once per ray.
-__device__ __noinline__ void mixed_finish(const DevParams& P, const DevOutputs& O, MixedSmem K,
+template <class KS>
+__device__ __noinline__ void mixed_finish(const DevParams& P, const DevOutputs& O, KS K,
                                           MixedRegs S, int cls, uint32_t n_att, uint32_t n_acc,
                                           bool crossed, BlockStats* bs) {
   const Ray R = mixed_fp64(K, S);
@@ -85,8 +88,9 @@ __device__ __noinline__ void mixed_finish(const DevParams& P, const DevOutputs& 
 // the pre-step state in FP64 (B), the increments and the seven stage
 // derivatives in this lane's shared-memory column (no step record in local
 // memory).
+template <class KS>
 struct MixedSpan {
-  MixedSmem K;
+  KS K;
   Ray B;
   double h;
   GG_DEV double xb(int c) const { return B.x[c]; }
@@ -105,13 +109,13 @@ struct MixedSpan {
 // the crossing; the next attempt would only find r > max_radius and return
 // Escaped, and is counted) -- writes its outcome and returns the attempts it
 // ended with, else 0.
-template <int METRIC, int DISK>
-__device__ __noinline__ uint32_t mixed_crossings(const DevParams& P, const DevOutputs& O, MixedSmem K,
+template <int METRIC, int DISK, class KS>
+__device__ __noinline__ uint32_t mixed_crossings(const DevParams& P, const DevOutputs& O, KS K,
                                              MixedRegs S, float hf, bool esc, bool dsk,
                                              uint32_t n_att, uint32_t n_acc, BlockStats* bs) {
   const Ray B = mixed_fp64(K, S);
   const uint64_t idx = K.idx();
-  const MixedSpan sp{K, B, (double)hf};
+  const MixedSpan<KS> sp{K, B, (double)hf};
   bool esc_end = false;
   double sky_th = 0.0, sky_ph = 0.0;
   if (esc && (O.cross || P.sky == kSkyChecker)) {
@@ -183,17 +187,19 @@ constexpr uint32_t kPendClsShift = 8;                  // kPendFinish: the class
 // (attempts between refills) and MINB (CTAs per SM the registers are
 // budgeted for) are the settings the batch autotuner chooses between.
 // SRC: kSrcCamera starts the samples from the camera; kSrcQueue continues the
-// rays the FP64 pass handed back (O.ret, ctl->returned of them).
-template <int METRIC, int DISK, bool BUDGET, bool BATCH, int PERIOD, int MINB, int SRC>
-__global__ void __launch_bounds__(kTraceBlock, MINB)
+// rays the FP64 pass handed back (O.ret, ctl->returned of them).  BLOCK
+// (threads per CTA) and CHUNK (samples a warp claims from the work queue at
+// a time) are the batch autotuner's other two settings.  The CTA's column
+// (mixed_smem_bytes<BLOCK>) is dynamic shared memory.
+template <int METRIC, int DISK, bool BUDGET, bool BATCH, int PERIOD, int MINB, int SRC,
+          int BLOCK = kTraceBlock, int CHUNK = (int)kChunk>
+__global__ void __launch_bounds__(BLOCK, MINB)
     trace_mixed_kernel(const __grid_constant__ DevParams P, const __grid_constant__ DevOutputs O,
                        DevControl* ctl, const __grid_constant__ BatchTable B) {
   const unsigned lane = threadIdx.x & 31u;
   __shared__ BlockStats bs;
-  __shared__ float4 k_smem[kMixedSlots][kTraceBlock];
-  __shared__ double lam_smem[kTraceBlock];
-  __shared__ uint64_t idx_smem[kTraceBlock];
-  const MixedSmem K{k_smem, lam_smem, idx_smem};
+  extern __shared__ __align__(16) unsigned char mixed_smem[];
+  const MixedSmemT<BLOCK> K = MixedSmemT<BLOCK>::at(mixed_smem);
   if (threadIdx.x < sizeof(BlockStats) / 8)
     reinterpret_cast<unsigned long long*>(&bs)[threadIdx.x] = 0ull;
   __syncthreads();
@@ -259,7 +265,7 @@ __global__ void __launch_bounds__(kTraceBlock, MINB)
       if (wcount == 0) {
         unsigned long long b = 0;
         if (lane == 0) {
-          b = atomicAdd(head, (unsigned long long)kChunk);
+          b = atomicAdd(head, (unsigned long long)CHUNK);
           if (BUDGET) {
             const unsigned long long used = atomicAdd(&ctl->budget_used, 0ull);
             if (used > P.attempt_budget) {
@@ -275,7 +281,7 @@ __global__ void __launch_bounds__(kTraceBlock, MINB)
         }
         wbase = b;
         const uint64_t left = n_src - b;
-        wcount = left < kChunk ? (uint32_t)left : kChunk;
+        wcount = left < (uint64_t)CHUNK ? (uint32_t)left : (uint32_t)CHUNK;
       }
       const unsigned nn = (unsigned)__popc(need);
       const unsigned take = nn < wcount ? nn : wcount;
@@ -398,15 +404,24 @@ __global__ void __launch_bounds__(kTraceBlock, MINB)
   }
 }
 
+// A kernel of the mixed form with its block size and dynamic shared memory.
+struct MixedKernel {
+  const void* fn;
+  int block;
+  int smem;
+};
+
 template <int METRIC, int DISK, bool BUDGET, bool BATCH = false, int PERIOD = kMixedPeriod,
-          int MINB = kMixedMinBlocks, int SRC = kSrcCamera>
-const void* mixed_fn() {
-  return reinterpret_cast<const void*>(
-      &trace_mixed_kernel<METRIC, DISK, BUDGET, BATCH, PERIOD, MINB, SRC>);
+          int MINB = kMixedMinBlocks, int SRC = kSrcCamera, int BLOCK = kTraceBlock,
+          int CHUNK = (int)kChunk>
+MixedKernel mixed_fn() {
+  return {reinterpret_cast<const void*>(
+              &trace_mixed_kernel<METRIC, DISK, BUDGET, BATCH, PERIOD, MINB, SRC, BLOCK, CHUNK>),
+          BLOCK, mixed_smem_bytes<BLOCK>()};
 }
 
 template <bool BUDGET>
-const void* select_mixed_disk(const DevParams& P) {
+MixedKernel select_mixed_disk(const DevParams& P) {
   if (P.metric == kMetricKerr)
     return P.disk == kDiskThin ? mixed_fn<kMetricKerr, kDiskThin, BUDGET>()
                                : mixed_fn<kMetricKerr, kDiskNone, BUDGET>();
@@ -417,7 +432,7 @@ const void* select_mixed_disk(const DevParams& P) {
 // The pass over the rays the FP64 pass handed back (no attempt budget: the
 // hand-back is off in budgeted renders).
 template <bool BATCH>
-const void* select_returned(const DevParams& P) {
+MixedKernel select_returned(const DevParams& P) {
   constexpr int Pd = kMixedPeriod, Mb = kMixedMinBlocksReturned;
   if (P.metric == kMetricKerr)
     return P.disk == kDiskThin
@@ -428,29 +443,35 @@ const void* select_returned(const DevParams& P) {
              : mixed_fn<kMetricSchwarzschild, kDiskNone, false, BATCH, Pd, Mb, kSrcQueue>();
 }
 
-// Batched launches: the variant (PERIOD, MINB) by index, kBatchVariants of
-// them; the metric and disk kind are the batch's.
-template <int METRIC, int DISK>
-const void* batch_variant(int v) {
-  switch (v) {
-    case 0: return mixed_fn<METRIC, DISK, false, true, 16, 8>();
-    case 1: return mixed_fn<METRIC, DISK, false, true, 8, 8>();
-    case 2: return mixed_fn<METRIC, DISK, false, true, 4, 8>();
-    case 3: return mixed_fn<METRIC, DISK, false, true, 16, 7>();
-    case 4: return mixed_fn<METRIC, DISK, false, true, 32, 7>();
-    default: return mixed_fn<METRIC, DISK, false, true, 32, 8>();
-  }
+// Batched launches: variant v of kBatchVariantTable (refill period, CTAs per
+// SM the registers are budgeted for, threads per CTA, samples per queue
+// claim); the metric and disk kind are the batch's.
+template <int METRIC, int DISK, int V>
+MixedKernel batch_v() {
+  constexpr BatchVariant b = kBatchVariantTable[V];
+  return mixed_fn<METRIC, DISK, false, true, b.period, b.ctas_per_sm, kSrcCamera, b.block,
+                  b.chunk>();
 }
 
-const void* select_batch(const DevParams& P, int v) {
+template <int METRIC, int DISK, int... Vs>
+MixedKernel batch_variant(int v, std::integer_sequence<int, Vs...>) {
+  MixedKernel k{nullptr, 0, 0};
+  ((v == Vs ? (k = batch_v<METRIC, DISK, Vs>(), 0) : 0), ...);
+  return k.fn ? k : batch_v<METRIC, DISK, 0>();
+}
+
+MixedKernel select_batch(const DevParams& P, int v) {
+  const auto all = std::make_integer_sequence<int, kBatchVariants>{};
   if (P.metric == kMetricKerr)
-    return P.disk == kDiskThin ? batch_variant<kMetricKerr, kDiskThin>(v)
-                               : batch_variant<kMetricKerr, kDiskNone>(v);
-  return P.disk == kDiskThin ? batch_variant<kMetricSchwarzschild, kDiskThin>(v)
-                             : batch_variant<kMetricSchwarzschild, kDiskNone>(v);
+    return P.disk == kDiskThin ? batch_variant<kMetricKerr, kDiskThin>(v, all)
+                               : batch_variant<kMetricKerr, kDiskNone>(v, all);
+  return P.disk == kDiskThin ? batch_variant<kMetricSchwarzschild, kDiskThin>(v, all)
+                             : batch_variant<kMetricSchwarzschild, kDiskNone>(v, all);
 }
 
-const void* select_mixed(const DevParams& P, const BatchTable* batch, int variant) {
+MixedKernel select_kernel(const DevParams& P, const BatchTable* batch, int variant,
+                          bool returned) {
+  if (returned) return batch ? select_returned<true>(P) : select_returned<false>(P);
   if (batch) return select_batch(P, variant);
   return P.attempt_budget ? select_mixed_disk<true>(P) : select_mixed_disk<false>(P);
 }
@@ -459,22 +480,25 @@ const void* select_mixed(const DevParams& P, const BatchTable* batch, int varian
 
 cudaError_t mixed_occupancy(const DevParams& P, int* blocks_per_sm, const BatchTable* batch,
                             int variant, bool returned) {
-  const void* fn = returned ? (batch ? select_returned<true>(P) : select_returned<false>(P))
-                            : select_mixed(P, batch, variant);
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, fn, kTraceBlock, 0);
+  const MixedKernel k = select_kernel(P, batch, variant, returned);
+  // opts in to more than 48 KB of dynamic shared memory where a variant
+  // needs it (idempotent; launches follow an occupancy query)
+  const cudaError_t e =
+      cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, k.smem);
+  if (e != cudaSuccess) return e;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k.fn, k.block, k.smem);
 }
 
 cudaError_t launch_mixed(const DevParams& P, const DevOutputs& O, DevControl* ctl, int grid,
                          cudaStream_t stream, const BatchTable* batch, int variant,
                          bool returned) {
-  const void* fn = returned ? (batch ? select_returned<true>(P) : select_returned<false>(P))
-                            : select_mixed(P, batch, variant);
+  const MixedKernel k = select_kernel(P, batch, variant, returned);
   DevParams p = P;
   DevOutputs o = O;
   BatchTable b{};
   if (batch) b = *batch;
   void* args[] = {&p, &o, &ctl, &b};
-  return cudaLaunchKernel(fn, dim3(grid), dim3(kTraceBlock), args, 0, stream);
+  return cudaLaunchKernel(k.fn, dim3(grid), dim3(k.block), args, k.smem, stream);
 }
 
 }  // namespace gg

@@ -111,8 +111,15 @@ GG_DEV void split(double x, float& hi, float& lo) {
 // dx, dv; 9 and 10 the position hi and lo parts; 11 the velocity lo part.
 constexpr int kSlotDx = 7, kSlotDv = 8, kSlotXh = 9, kSlotXl = 10, kSlotVl = 11;
 constexpr int kMixedSlots = 12;
-struct MixedSmem {
-  float4 (*s)[kTraceBlock];
+// Shared memory of a CTA of BLOCK threads: the slots, then the affine
+// parameters and sample indices.
+template <int BLOCK>
+constexpr int mixed_smem_bytes() {
+  return kMixedSlots * BLOCK * (int)sizeof(float4) + BLOCK * (int)(sizeof(double) + 8);
+}
+template <int BLOCK>
+struct MixedSmemT {
+  float4 (*s)[BLOCK];
   double* lam_s;
   uint64_t* idx_s;
   GG_DEV float4 get(int slot) const { return s[slot][threadIdx.x]; }
@@ -122,7 +129,15 @@ struct MixedSmem {
   }
   GG_DEV double& lam() const { return lam_s[threadIdx.x]; }
   GG_DEV uint64_t& idx() const { return idx_s[threadIdx.x]; }
+  // the column laid out in a CTA's dynamic shared memory
+  GG_DEV static MixedSmemT at(void* smem) {
+    auto* k = reinterpret_cast<float4(*)[BLOCK]>(smem);
+    auto* lam = reinterpret_cast<double*>(reinterpret_cast<char*>(smem) +
+                                          kMixedSlots * BLOCK * sizeof(float4));
+    return {k, lam, reinterpret_cast<uint64_t*>(lam + BLOCK)};
+  }
 };
+using MixedSmem = MixedSmemT<kTraceBlock>;
 
 // Register part of a mixed-form ray.
 struct MixedRegs {
@@ -131,7 +146,8 @@ struct MixedRegs {
 };
 
 // Starts a ray: state from FP64, split into hi + lo.
-GG_DEV void mixed_load(const Ray& R, uint64_t idx, const MixedSmem& K, MixedRegs& S) {
+template <class KS>
+GG_DEV void mixed_load(const Ray& R, uint64_t idx, const KS& K, MixedRegs& S) {
   float xh[4], xl[4], vl[4];
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
@@ -147,7 +163,8 @@ GG_DEV void mixed_load(const Ray& R, uint64_t idx, const MixedSmem& K, MixedRegs
 }
 
 // The ray's state in FP64 (hi + lo).
-GG_DEV Ray mixed_fp64(const MixedSmem& K, const MixedRegs& S) {
+template <class KS>
+GG_DEV Ray mixed_fp64(const KS& K, const MixedRegs& S) {
   const float4 xh = K.get(kSlotXh), xl = K.get(kSlotXl), vl = K.get(kSlotVl);
   Ray R;
   R.x[0] = (double)xh.x + (double)xl.x;
@@ -181,8 +198,8 @@ struct DPa {
 };
 
 // ax += sum_l Abar[S][l] k_l, av += sum_l B[S][l] k_l over l < S.
-template <int S, int L>
-GG_DEV void stage_sums(const MixedSmem& K, float ax[4], float av[4]) {
+template <int S, int L, class KS>
+GG_DEV void stage_sums(const KS& K, float ax[4], float av[4]) {
   if constexpr (L < S) {
     constexpr float cb = DPc<S, L>::abar, cv = DPc<S, L>::b;
     if constexpr (cb != 0.0f || cv != 0.0f) {
@@ -199,8 +216,8 @@ GG_DEV void stage_sums(const MixedSmem& K, float ax[4], float av[4]) {
 }
 
 // ex += sum_l Ebar_l k_l, ev += sum_l E_l k_l over the seven stages.
-template <int L>
-GG_DEV void error_sums(const MixedSmem& K, float ex[4], float ev[4]) {
+template <int L, class KS>
+GG_DEV void error_sums(const KS& K, float ex[4], float ev[4]) {
   if constexpr (L < 7) {
     constexpr float eb = DPe<L>::ebar, e = DPe<L>::e;
     if constexpr (eb != 0.0f || e != 0.0f) {
@@ -218,8 +235,8 @@ GG_DEV void error_sums(const MixedSmem& K, float ex[4], float ev[4]) {
 
 // The same sums in FP64 over the FP32 stage derivatives (each product and
 // sum carries the FP64 rounding only), the coefficients in FP64.
-template <int L>
-GG_DEV void error_sums64(const MixedSmem& K, double ex[4], double ev[4]) {
+template <int L, class KS>
+GG_DEV void error_sums64(const KS& K, double ex[4], double ev[4]) {
   if constexpr (L < 7) {
     constexpr double eb = make_dp_table().Ebar[L], e = make_dp_table().E[L];
     if constexpr (eb != 0.0 || e != 0.0) {
@@ -239,8 +256,8 @@ GG_DEV void error_sums64(const MixedSmem& K, double ex[4], double ev[4]) {
 // x_S = x + h a_S v + h^2 sum Abar k, v_S = v + h sum B k.  Stage 6 is the
 // 5th-order solution: its four position and velocity increments are the
 // step's dx, dv (slots 7, 8).
-template <int S>
-GG_DEV void mixed_stage(float r0, float th0, const MixedRegs& st, const MixedSmem& K, float hf,
+template <int S, class KS>
+GG_DEV void mixed_stage(float r0, float th0, const MixedRegs& st, const KS& K, float hf,
                         float hh, float& pr, float& pth, float pw[4]) {
   float ax[4] = {0.0f, 0.0f, 0.0f, 0.0f}, av[4] = {0.0f, 0.0f, 0.0f, 0.0f};
   stage_sums<S, 0>(K, ax, av);
@@ -373,7 +390,8 @@ GG_DEV double fifth_root_accept(double x) {
 
 // The escape test of the reference's step (geodesic.rs:195-197) on the
 // float-pair radius.
-GG_DEV bool beyond_max_radius(const DevParams& P, const MixedSmem& K) {
+template <class KS>
+GG_DEV bool beyond_max_radius(const DevParams& P, const KS& K) {
   return ff_minus(K.comp(kSlotXh, 1), K.comp(kSlotXl, 1), P.max_radius_hi, P.max_radius_lo) >
          0.0f;
 }
@@ -386,8 +404,8 @@ GG_DEV bool beyond_max_radius(const DevParams& P, const MixedSmem& K) {
 // (mixed_advance applies it).  The horizon test never fires here: the FP64
 // band starts 0.5 M outside the horizon and its buffer.  Invalid stages are
 // judged on r and theta, the coordinates the stages form.
-template <int METRIC>
-GG_DEV int attempt_dp45_mixed(const DevParams& P, MixedRegs& S, const MixedSmem& K,
+template <int METRIC, class KS>
+GG_DEV int attempt_dp45_mixed(const DevParams& P, MixedRegs& S, const KS& K,
                               bool& k1_valid, bool& k7_pending, bool& accepted, float& hf) {
   accepted = false;
   if (beyond_max_radius(P, K)) return kEscaped;
@@ -521,7 +539,8 @@ GG_DEV int attempt_dp45_mixed(const DevParams& P, MixedRegs& S, const MixedSmem&
 
 // Applies an accepted attempt's increments (compensated) and wraps phi into
 // [0, 2 pi); k7 becomes the next attempt's k1.
-GG_DEV void mixed_advance(MixedRegs& S, const MixedSmem& K, float hf, bool& k1_valid,
+template <class KS>
+GG_DEV void mixed_advance(MixedRegs& S, const KS& K, float hf, bool& k1_valid,
                           bool& k7_pending) {
   const float4 dx4 = K.get(kSlotDx), dv4 = K.get(kSlotDv);
   const float4 xh4 = K.get(kSlotXh), xl4 = K.get(kSlotXl), vl4 = K.get(kSlotVl);

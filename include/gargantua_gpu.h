@@ -283,7 +283,7 @@ typedef struct gg_scene_t {
   uint64_t sky_seed; /* checkerboard seed of this scene                      */
 } gg_scene_t;
 
-#define GG_BATCH_VARIANTS 6 /* kernel variants the batch autotuner chooses from */
+#define GG_BATCH_VARIANTS 12 /* kernel variants the batch autotuner chooses from */
 
 /* Renders n scenes in one persistent launch of the mixed-precision kernel
  * (integ: GG_PREC_MIXED, GG_STEPPER_DP45; opts: one sample per pixel), its
@@ -292,9 +292,10 @@ typedef struct gg_scene_t {
  * (scene count, total samples, integrator and options) and replayed; the
  * scenes' parameters are uploaded from the context's pinned buffer by a copy
  * node inside the graph, so a batch of the same shape with new cameras,
- * spins or disks reuses the graph.  The kernel variant (compaction period x
- * register budget) is the one gg_batch_autotune chose on this context, or a
- * fixed default.
+ * spins or disks reuses the graph.  The kernel variant (compaction period,
+ * register budget, threads per CTA and samples per work-queue claim; see
+ * gg_batch_variant_info) is the one gg_batch_autotune chose on this context,
+ * or a fixed default.
  * gg_render_batch_device: images concatenated in scene order into rgb_dev
  * (scene k at byte 3 * sum_{j<k} w_j h_j), enqueued on `stream` (NULL = CUDA's
  * default stream).  gg_render_batch: synchronous, rgb_out[k] = scene k's
@@ -314,6 +315,11 @@ GG_API int gg_batch_autotune(gg_ctx* ctx, const gg_scene_t* scenes, uint32_t n,
                              int* variant_out, double* ms_out);
 /* Sets the context's batch kernel variant (0 .. GG_BATCH_VARIANTS-1). */
 GG_API int gg_batch_set_variant(gg_ctx* ctx, int variant);
+/* The settings of batch kernel variant v: out[0] refill period (attempts
+ * between a warp's refills), out[1] CTAs per SM its registers are budgeted
+ * for, out[2] threads per CTA, out[3] samples a warp claims from the work
+ * queue at a time.  0, or GG_ERR_INVALID_ARG.  Host only; no device needed. */
+GG_API int gg_batch_variant_info(int v, int32_t out[4]);
 
 /* ---- differentiable render (no reference counterpart) ------------------- */
 /* Forward pass of the differentiable render: Kerr (metric), the inclined

@@ -32,6 +32,24 @@ def test_batch_scene_generator_ranges_and_determinism():
     assert workloads.batch_scenes(4, seed=1)[0].metric.spin != a[0].metric.spin
 
 
+def test_batch_variant_table(gglib):
+    """The autotuner's grid: refill period, register budget, block size (64,
+    128, 256 threads) and samples per queue claim (16, 32, 64), each variant
+    within the SM's 2,048 threads and 228 KB of shared memory (12 slots of
+    16 B plus 16 B per thread, 1 KB reserved per CTA)."""
+    vs = [abi.batch_variant(v) for v in range(abi.GG_BATCH_VARIANTS)]
+    assert len(set(vs)) == len(vs)
+    assert {v[2] for v in vs} == {64, 128, 256} and {v[3] for v in vs} == {16, 32, 64}
+    for period, ctas, block, chunk in vs:
+        assert period in (4, 8, 16, 32) and block % 32 == 0
+        assert block * ctas <= 2048
+        assert 65536 // (block * ctas) >= 64  # registers per thread
+        assert ctas * (block * (12 * 16 + 16) + 1024 + 128) <= 228 * 1024
+    with pytest.raises(abi.GargantuaError):
+        abi.batch_variant(abi.GG_BATCH_VARIANTS)
+    assert len(abi.batch_variant_names()) == abi.GG_BATCH_VARIANTS
+
+
 def _small_batch(n=6):
     return workloads.batch_scenes(n, seed=3, max_side=128)
 
