@@ -24,10 +24,10 @@
 //   2. every earlier step in reverse, segment by segment: the segment is
 //      replayed from its checkpoint (the controller is deterministic, so the
 //      replay takes the same steps), then the adjoint goes back through each
-//      step's Dormand-Prince stages (vector-Jacobian products; each stage's
-//      4 x 7 Jacobian in r, theta, the stage velocity and the spin from a
-//      7-direction dual evaluation of the same Kerr right-hand side), with
-//      theta reflections at the poles reversing its adjoint;
+//      step's Dormand-Prince stages (vector-Jacobian products of each
+//      stage's Kerr right-hand side in r, theta, the stage velocity and the
+//      spin, by a hand-written reverse pass, gg_vjp.cuh), with theta
+//      reflections at the poles reversing its adjoint;
 //   3. the camera: the initial state and the observer normalisation as
 //      3-direction duals in (a, inclination, r_cam), contracted with the
 //      adjoint of the initial state.
@@ -40,8 +40,25 @@
 
 #include "gg_device.cuh"
 #include "gg_dual.cuh"
+#include "gg_vjp.cuh"
 #include "gg_launch.h"
 #include "gg_trace_common.cuh"
+
+// Build knobs of the backward (tuning builds compare them).  GG_ADJ_HAND_VJP:
+// each stage's vector-Jacobian product by the hand-written reverse pass
+// (kerr_rhs_vjp_hand) instead of dual numbers.  GG_ADJ_STORE_K: the replay
+// keeps each accepted step's stage derivatives for the step's product instead
+// of evaluating them again.  GG_ADJ_MIN_BLOCKS: the CTAs per SM the backward's
+// registers are budgeted for (1 leaves the compiler's own choice).
+#ifndef GG_ADJ_HAND_VJP
+#define GG_ADJ_HAND_VJP 1
+#endif
+#ifndef GG_ADJ_STORE_K
+#define GG_ADJ_STORE_K 1
+#endif
+#ifndef GG_ADJ_MIN_BLOCKS
+#define GG_ADJ_MIN_BLOCKS 1
+#endif
 
 namespace gg {
 
@@ -56,55 +73,6 @@ GG_DEV void kerr_rhs_dual(double M, const Dual<N>& a, const Dual<N>& r, const Du
   sincos(th, &s, &c);
   const KerrGeo<Dual<N>> G = kerr_geometry<Dual<N>>(Dual<N>(M), a, r, s, c);
   kerr_contract<Dual<N>>(G, w, acc);
-}
-
-// Vector-Jacobian product of one Kerr right-hand side a^mu(r, theta, w; spin)
-// with the cotangent kb: Xr, Xth, W[4] and (accumulated) *ga are kb . da/dr,
-// da/dtheta, da/dw^m and da/dspin.  The geometry depends on (r, theta, spin)
-// only and the contraction is quadratic in w, so the r, theta and spin columns
-// come from a 3-direction dual evaluation with w held constant, and the w
-// columns from a 4-direction dual of the contraction alone with the
-// geometry's values held constant.  Each direction's arithmetic is the one
-// a single 7-direction evaluation would do (the terms dropped are exact
-// zeros), at about half its cost.
-GG_DEV void kerr_rhs_vjp(double M, double spin, double r, double th, const double w[4],
-                         const double kb[4], double* Xr, double* Xth, double W[4], double* ga) {
-  Dual<3> s, c;
-  sincos(Dual<3>::var(th, 1), &s, &c);
-  const KerrGeo<Dual<3>> G =
-      kerr_geometry<Dual<3>>(Dual<3>(M), Dual<3>::var(spin, 2), Dual<3>::var(r, 0), s, c);
-  Dual<3> w3[4], acc3[4];
-#pragma unroll
-  for (int i = 0; i < 4; ++i) w3[i] = Dual<3>(w[i]);
-  kerr_contract<Dual<3>>(G, w3, acc3);
-  KerrGeo<Dual<4>> Gv;  // the geometry's values, constant in w
-  Gv.dtt_r = G.dtt_r.v;
-  Gv.dtt_th = G.dtt_th.v;
-  Gv.drr_r = G.drr_r.v;
-  Gv.drr_th = G.drr_th.v;
-  Gv.dthth_r = G.dthth_r.v;
-  Gv.dthth_th = G.dthth_th.v;
-  Gv.dphph_r = G.dphph_r.v;
-  Gv.dphph_th = G.dphph_th.v;
-  Gv.dtph_r = G.dtph_r.v;
-  Gv.dtph_th = G.dtph_th.v;
-  Gv.gtt = G.gtt.v;
-  Gv.gtph = G.gtph.v;
-  Gv.gphph = G.gphph.v;
-  Gv.hrr = G.hrr.v;
-  Gv.hthth = G.hthth.v;
-  Dual<4> w4[4], acc4[4];
-#pragma unroll
-  for (int i = 0; i < 4; ++i) w4[i] = Dual<4>::var(w[i], i);
-  kerr_contract<Dual<4>>(Gv, w4, acc4);
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    *Xr += acc3[i].d[0] * kb[i];
-    *Xth += acc3[i].d[1] * kb[i];
-#pragma unroll
-    for (int m = 0; m < 4; ++m) W[m] += acc4[i].d[m] * kb[i];
-    *ga += acc3[i].d[2] * kb[i];
-  }
 }
 
 // g of a Keplerian emitter at the equator (redshift_factor at theta = pi/2)
@@ -129,8 +97,10 @@ GG_DEV T redshift_eq(double M, const T& a, const T& r, const T v[4]) {
 // Vector-Jacobian product through one accepted full Dormand-Prince step
 // (Nystrom form, attempt_dp45_fp64): (lx, lv) is dL/d(x_new, v_new) on entry
 // and dL/d(x, v) on return; dL/da is accumulated into *ga.
+// kst: the step's stage derivatives k_1..k_6 as the forward took them, or
+// null to evaluate them again here.
 GG_DEV void dp45_vjp(const DevParams& P, const double x[4], const double v[4], double h,
-                     double lx[4], double lv[4], double* ga) {
+                     const double (*kst)[4], double lx[4], double lv[4], double* ga) {
   double k[6][4], pr[6], pth[6], pw[6][4];
   const double hh = h * h;
   for (int s = 0; s < 6; ++s) {
@@ -146,9 +116,14 @@ GG_DEV void dp45_vjp(const DevParams& P, const double x[4], const double v[4], d
         px[i] = fma(hh * kDP.Abar[s][l], k[l][i], px[i]);
         w[i] = fma(h * kDP.B[s][l], k[l][i], w[i]);
       }
-    Geometry<kMetricKerr> G;
-    G.at(P, px[1], px[2]);
-    G.accel(w, k[s]);
+    if (kst) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i) k[s][i] = kst[s][i];
+    } else {
+      Geometry<kMetricKerr> G;
+      G.at(P, px[1], px[2]);
+      G.accel(w, k[s]);
+    }
     pr[s] = px[1];
     pth[s] = px[2];
 #pragma unroll
@@ -171,7 +146,11 @@ GG_DEV void dp45_vjp(const DevParams& P, const double x[4], const double v[4], d
   for (int s = 5; s >= 0; --s) {
     // k_s = f(r_s, theta_s, w_s; a), back through its Jacobian
     double Xr = 0.0, Xth = 0.0, W[4] = {0.0, 0.0, 0.0, 0.0};
-    kerr_rhs_vjp(P.mass, P.spin, pr[s], pth[s], pw[s], kb[s], &Xr, &Xth, W, ga);
+#if GG_ADJ_HAND_VJP
+    kerr_rhs_vjp_hand(P.mass, P.spin, pr[s], pth[s], pw[s], kb[s], &Xr, &Xth, W, ga);
+#else
+    kerr_rhs_vjp_dual(P.mass, P.spin, pr[s], pth[s], pw[s], kb[s], &Xr, &Xth, W, ga);
+#endif
     // x_s = x + h A_s v + h^2 sum_{l<s} Abar k_l ; w_s = v + h sum_{l<s} B k_l
     xbar[1] += Xr;
     xbar[2] += Xth;
@@ -358,9 +337,10 @@ GG_DEV void camera_dual(const DevParams& P, double u, double v, Dual<3> y0[8], D
 }
 
 // Replays one segment of accepted steps from a checkpoint, recording each
-// step's start state, size and whether its end was reflected at a pole.
+// step's start state, size and whether its end was reflected at a pole, and
+// (Kst non-null) its stage derivatives k_1..k_6.
 GG_DEV void replay(const DevParams& P, const Ckpt& c0, uint32_t steps, double S[][8], double* H,
-                   uint32_t* refl) {
+                   double (*Kst)[6][4], uint32_t* refl) {
   double kl[7][4];
   const KStoreLocal K{kl};
   Ray R;
@@ -392,6 +372,10 @@ GG_DEV void replay(const DevParams& P, const Ckpt& c0, uint32_t steps, double S[
           S[j][4 + i] = vb[i];
         }
         H[j] = h_used;
+        if (Kst)
+          for (int l = 0; l < 6; ++l)
+#pragma unroll
+            for (int i = 0; i < 4; ++i) Kst[j][l][i] = kl[l][i];
         if (end.xraw[2] < 0.0 || end.xraw[2] > kPi) *refl |= 1u << j;
         break;
       }
@@ -412,6 +396,11 @@ GG_DEV void backward_ray(const DevParams& P, const DiffOut& D, const double* dl_
   double lam[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   double ga = 0.0, g_rin = 0.0, g_q = 0.0, g_sobs = 0.0;
   double S[kCkptEvery][8], H[kCkptEvery];
+#if GG_ADJ_STORE_K
+  double Kst[kCkptEvery][6][4];
+#else
+  double (*Kst)[6][4] = nullptr;
+#endif
   bool ok = true;
   for (int seg = (int)n_ck - 1; seg >= 0 && ok; --seg) {
     const uint32_t first = (uint32_t)seg * kCkptEvery;
@@ -421,7 +410,7 @@ GG_DEV void backward_ray(const DevParams& P, const DiffOut& D, const double* dl_
       break;
     }
     uint32_t refl = 0;
-    replay(P, ck[seg], steps, S, H, &refl);
+    replay(P, ck[seg], steps, S, H, Kst, &refl);
     for (int j = (int)steps - 1; j >= 0; --j) {
       if (seg == (int)n_ck - 1 && j == (int)steps - 1) {
         ok = crossing_vjp(P, S[j], S[j] + 4, H[j], dl, lam, &ga, &g_rin, &g_q, &g_sobs);
@@ -429,7 +418,7 @@ GG_DEV void backward_ray(const DevParams& P, const DiffOut& D, const double* dl_
         continue;
       }
       if (refl & (1u << j)) lam[2] = -lam[2];  // theta -> -theta or 2 pi - theta
-      dp45_vjp(P, S[j], S[j] + 4, H[j], lam, lam + 4, &ga);
+      dp45_vjp(P, S[j], S[j] + 4, H[j], Kst ? Kst[j] : nullptr, lam, lam + 4, &ga);
     }
   }
   if (!ok) return;
@@ -542,7 +531,7 @@ __global__ void backward_scatter_kernel(const __grid_constant__ DevParams P,
 }
 
 // Persistent: each warp claims the next 32 entries of the sorted list.
-__global__ void __launch_bounds__(128) diff_backward_kernel(const __grid_constant__ DevParams P,
+__global__ void __launch_bounds__(128, GG_ADJ_MIN_BLOCKS) diff_backward_kernel(const __grid_constant__ DevParams P,
                                                             const __grid_constant__ DiffOut D,
                                                             const double* dl_drgb,
                                                             double* grad5, BackwardList L) {

@@ -13,6 +13,7 @@
 
 #include "../../include/gargantua_gpu.h"
 #include "gg_device.cuh"
+#include "gg_vjp.cuh"
 
 namespace {
 
@@ -34,6 +35,31 @@ __global__ void spatial_dir_kernel(const double* __restrict__ vel, double* __res
        i += (uint64_t)gridDim.x * blockDim.x) {
     const double v[4] = {vel[4 * i], vel[4 * i + 1], vel[4 * i + 2], vel[4 * i + 3]};
     gg::spatial_dir(v, dirs[3 * i], dirs[3 * i + 1], dirs[3 * i + 2]);
+  }
+}
+
+// 12 doubles in per point (M, a, r, theta, w[4], kb[4]); 7 out (kb . da/dr,
+// da/dtheta, da/dw[4], da/da).
+__global__ void kerr_vjp_kernel(const double* __restrict__ in, double* __restrict__ out,
+                                uint64_t n, int form) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const double* q = in + 12 * i;
+    const double w[4] = {q[4], q[5], q[6], q[7]};
+    const double kb[4] = {q[8], q[9], q[10], q[11]};
+    double Xr = 0.0, Xth = 0.0, W[4] = {0.0, 0.0, 0.0, 0.0}, ga = 0.0;
+    if (form == 0)
+      gg::kerr_rhs_vjp_hand(q[0], q[1], q[2], q[3], w, kb, &Xr, &Xth, W, &ga);
+    else
+      gg::kerr_rhs_vjp_dual(q[0], q[1], q[2], q[3], w, kb, &Xr, &Xth, W, &ga);
+    double* o = out + 7 * i;
+    o[0] = Xr;
+    o[1] = Xth;
+    o[2] = W[0];
+    o[3] = W[1];
+    o[4] = W[2];
+    o[5] = W[3];
+    o[6] = ga;
   }
 }
 
@@ -61,5 +87,15 @@ extern "C" GG_API int gg_check_spatial_dir(const double* vel_dev, double* dirs_d
   const uint64_t blocks = (n + 255) / 256;
   spatial_dir_kernel<<<(unsigned)(blocks < 4096 ? blocks : 4096), 256, 0,
                        static_cast<cudaStream_t>(stream)>>>(vel_dev, dirs_dev, n);
+  return launch_status();
+}
+
+extern "C" GG_API int gg_check_kerr_vjp(const double* in_dev, double* out_dev, uint64_t n,
+                                        int form, void* stream) {
+  if (n == 0) return GG_OK;
+  if (!in_dev || !out_dev || (form != 0 && form != 1)) return GG_ERR_INVALID_ARG;
+  const uint64_t blocks = (n + 127) / 128;
+  kerr_vjp_kernel<<<(unsigned)(blocks < 4096 ? blocks : 4096), 128, 0,
+                    static_cast<cudaStream_t>(stream)>>>(in_dev, out_dev, n, form);
   return launch_status();
 }

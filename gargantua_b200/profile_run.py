@@ -2,6 +2,7 @@
 
     python -m gargantua_b200.profile_run --workload kerr_thin_1080p --precision mixed
     python -m gargantua_b200.profile_run --workload adjoint_512 --repeats 3
+    python -m gargantua_b200.profile_run --workload adjoint_512 --side 128 --repeats 2
 
 Prints the device time and statistics of each render.  Under a profiler,
 select the trace launch with its kernel name (trace_mixed_kernel,
@@ -25,12 +26,15 @@ WORKLOADS = {
 }
 
 
-def run_adjoint(repeats: int) -> None:
+def run_adjoint(repeats: int, side: int | None = None) -> None:
     import torch
 
     from . import diff
     r = Renderer(0)
-    dr = diff.DiffRenderer(diff.DiffScene(), r)
+    scene = diff.DiffScene()
+    if side:
+        scene.width = scene.height = side
+    dr = diff.DiffRenderer(scene, r)
     target = dr.render(diff.target_params()).clone()
     p = diff.perturbed_params(0)
     stream = torch.cuda.current_stream()
@@ -43,7 +47,7 @@ def run_adjoint(repeats: int) -> None:
         g = dr.backward(dl.data_ptr(), stream.cuda_stream)
         e1.record(stream)
         stream.synchronize()
-        print(json.dumps({"workload": "adjoint_512", "gradient_ms": e0.elapsed_time(e1),
+        print(json.dumps({"workload": "adjoint_512", "side": scene.width, "gradient_ms": e0.elapsed_time(e1),
                           "forward_attempts": st.attempts, "gradient": [float(x) for x in g]}),
               flush=True)
     r.close()
@@ -56,7 +60,8 @@ def main() -> None:
     ap.add_argument("--stepper", choices=["reference", "dp45"], default=None,
                     help="default: dp45 for mixed, reference for fp64")
     ap.add_argument("--repeats", type=int, default=1)
-    ap.add_argument("--side", type=int, default=None, help="kerr_stress_4k: image side")
+    ap.add_argument("--side", type=int, default=None,
+                    help="kerr_stress_4k, adjoint_512: image side (a smaller case for profilers)")
     ap.add_argument("--spp", type=int, default=None, help="kerr_stress_4k: samples per pixel")
     ap.add_argument("--width", type=int, default=None,
                     help="render the same view at this width (with --height): a smaller case "
@@ -64,7 +69,7 @@ def main() -> None:
     ap.add_argument("--height", type=int, default=None)
     a = ap.parse_args()
     if a.workload == "adjoint_512":
-        run_adjoint(a.repeats)
+        run_adjoint(a.repeats, a.side)
         return
     prec = abi.GG_PREC_MIXED if a.precision == "mixed" else abi.GG_PREC_FP64
     stepper = a.stepper or ("dp45" if a.precision == "mixed" else "reference")

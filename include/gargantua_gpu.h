@@ -419,6 +419,15 @@ GG_API int gg_check_procedural_sky(const double* dirs_dev, double* rgb_dev, uint
 GG_API int gg_check_spatial_dir(const double* vel_dev, double* dirs_dev, uint64_t n,
                                 void* stream);
 
+/* Vector-Jacobian product of one Kerr right-hand side, the product the
+ * differentiable render's backward takes at every stage (test use; no
+ * reference counterpart).  in_dev: n points of 12 doubles (M, a, r, theta,
+ * w[4], kb[4]); out_dev: n x 7 (kb . da/dr, da/dtheta, da/dw[0..3], da/da).
+ * form 0: the hand-written reverse pass; 1: dual numbers.  Same pointer,
+ * stream and return conventions as above; GG_ERR_INVALID_ARG for another form. */
+GG_API int gg_check_kerr_vjp(const double* in_dev, double* out_dev, uint64_t n, int form,
+                             void* stream);
+
 #ifdef __cplusplus
 }
 #endif
