@@ -91,6 +91,28 @@ def test_batch_equals_single_scene_renders(renderer):
 
 
 @pytest.mark.gpu
+def test_batch_scenes_against_oracle(renderer, oracle_mod):
+    """The batch held to the FP64 oracle directly, not only through the
+    single-scene renders: each scene of a small batch (mixed precision)
+    against the oracle's render of the same scene with the same stepper in
+    FP64.  The batch returns images only, so the bar is on the bytes: within
+    one step of 255 on 99.9 % of the pixels, as the single mixed renders are
+    held to the FP64 kernel."""
+    scenes = workloads.batch_scenes(10, seed=4, max_side=256)
+    ref = workloads.batch_scenes(10, seed=4, max_side=256, precision=abi.GG_PREC_FP64)
+    imgs = renderer.render_batch(scenes)
+    close = exact = total = 0
+    for img, sc in zip(imgs, ref):
+        want, _ = oracle_mod.render(sc)
+        d = np.abs(img.astype(int) - want.astype(int)).max(axis=2)
+        close += int((d <= 1).sum())
+        exact += int((d == 0).sum())
+        total += d.size
+    assert close / total >= 0.999, (close, total)
+    assert exact / total >= 0.99, (exact, total)
+
+
+@pytest.mark.gpu
 def test_batch_graph_replay_with_new_parameters(renderer):
     scenes = _small_batch()
     first = renderer.render_batch(scenes)
