@@ -40,6 +40,12 @@
 // acceptance test and the step law on the squared norm s2 itself (s2 < 8;
 // h 0.9 (8 / s2)^(1/10)) instead of forming err = sqrt(s2 / 8), tol / err and
 // its fifth root: 26.35 against 26.95 ms, the same attempts to 20 in 416.6 M.
+// GG_MIXED_PAIRED (default) forms the stage sums with the paired FP32 fused
+// multiply-add and the accepted step's two-sum state update with the paired
+// add, two components per instruction: 25.7 against 26.5 ms, the same bits.
+// Pairing the contraction's r and theta rows the same way (26.6 ms) or the
+// stage-6 position increments (26.2 ms) gave the same bits too but cost more
+// in register moves and spills than they saved.
 #ifndef GG_MIXED_ERR_FP64
 #define GG_MIXED_ERR_FP64 1
 #endif
@@ -48,6 +54,9 @@
 #endif
 #ifndef GG_MIXED_ROOT10
 #define GG_MIXED_ROOT10 1
+#endif
+#ifndef GG_MIXED_PAIRED
+#define GG_MIXED_PAIRED 1
 #endif
 
 namespace gg {
@@ -97,6 +106,21 @@ GG_DEV void ff_add(float& hi, float& lo, float d) {
   hi = s + t;
   lo = t - (hi - s);
 }
+
+#if GG_MIXED_PAIRED
+// ff_add on two components at once with the paired FP32 add (a - b as
+// a + (-b), exact): the same operations per lane, so the same bits.
+GG_DEV float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+GG_DEV void ff_add2(float2& hi, float2& lo, float2 d) {
+  const float2 s = __fadd2_rn(hi, d);
+  const float2 bb = __fadd2_rn(s, neg2(hi));
+  const float2 e =
+      __fadd2_rn(__fadd2_rn(hi, neg2(__fadd2_rn(s, neg2(bb)))), __fadd2_rn(d, neg2(bb)));
+  const float2 t = __fadd2_rn(lo, e);
+  hi = __fadd2_rn(s, t);
+  lo = __fadd2_rn(t, neg2(__fadd2_rn(hi, neg2(s))));
+}
+#endif
 
 // (hi + lo) - (c_hi + c_lo) to FP32 accuracy, exact in its leading part when
 // hi is within a factor 2 of c_hi (Sterbenz): the sign tests of the escape
@@ -221,6 +245,44 @@ GG_DEV void stage_sums(const KS& K, float ax[4], float av[4]) {
   }
 }
 
+#if GG_MIXED_PAIRED
+// The same sums with the paired FP32 fused multiply-add (two lanes of one
+// instruction, each rounded as fmaf): the velocity sums over (t, r) and
+// (theta, phi), and, for stage 6 whose four position increments are all
+// used, the position sums too; stages 1-5 form only r and theta.  Same
+// operations in the same order, so the same bits as stage_sums.
+template <int S, int L, class KS>
+GG_DEV void stage_sums2(const KS& K, float ax[4], float2& av01, float2& av23) {
+  if constexpr (L < S) {
+    constexpr float cb = DPc<S, L>::abar, cv = DPc<S, L>::b;
+    if constexpr (cb != 0.0f || cv != 0.0f) {
+      const float4 k4 = K.get(L);
+      const float2 k01 = make_float2(k4.x, k4.y), k23 = make_float2(k4.z, k4.w);
+      if constexpr (cb != 0.0f) {
+        if constexpr (S == 6) {
+          const float2 c2 = make_float2(cb, cb);
+          const float2 a01 = __ffma2_rn(c2, k01, make_float2(ax[0], ax[1]));
+          const float2 a23 = __ffma2_rn(c2, k23, make_float2(ax[2], ax[3]));
+          ax[0] = a01.x;
+          ax[1] = a01.y;
+          ax[2] = a23.x;
+          ax[3] = a23.y;
+        } else {
+          ax[1] = fmaf(cb, k4.y, ax[1]);
+          ax[2] = fmaf(cb, k4.z, ax[2]);
+        }
+      }
+      if constexpr (cv != 0.0f) {
+        const float2 c2 = make_float2(cv, cv);
+        av01 = __ffma2_rn(c2, k01, av01);
+        av23 = __ffma2_rn(c2, k23, av23);
+      }
+    }
+    stage_sums2<S, L + 1>(K, ax, av01, av23);
+  }
+}
+#endif
+
 // ex += sum_l Ebar_l k_l, ev += sum_l E_l k_l over the seven stages.
 template <int L, class KS>
 GG_DEV void error_sums(const KS& K, float ex[4], float ev[4]) {
@@ -266,7 +328,29 @@ template <int S, class KS>
 GG_DEV void mixed_stage(float r0, float th0, const MixedRegs& st, const KS& K, float hf,
                         float hh, float& pr, float& pth, float pw[4]) {
   float ax[4] = {0.0f, 0.0f, 0.0f, 0.0f}, av[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#if GG_MIXED_PAIRED
+  float2 av01 = make_float2(0.0f, 0.0f), av23 = make_float2(0.0f, 0.0f);
+  stage_sums2<S, 0>(K, ax, av01, av23);
+  if constexpr (S != 6) {  // the stage velocity, paired: v + h sum B k
+    const float2 h2 = make_float2(hf, hf);
+    const float2 w01 = __ffma2_rn(h2, av01, make_float2(st.vh[0], st.vh[1]));
+    const float2 w23 = __ffma2_rn(h2, av23, make_float2(st.vh[2], st.vh[3]));
+    pw[0] = w01.x;
+    pw[1] = w01.y;
+    pw[2] = w23.x;
+    pw[3] = w23.y;
+    const float ha = hf * DPa<S>::a;
+    pr = r0 + fmaf(hh, ax[1], ha * st.vh[1]);
+    pth = th0 + fmaf(hh, ax[2], ha * st.vh[2]);
+    return;
+  }
+  av[0] = av01.x;
+  av[1] = av01.y;
+  av[2] = av23.x;
+  av[3] = av23.y;
+#else
   stage_sums<S, 0>(K, ax, av);
+#endif
   const float ha = hf * DPa<S>::a;
   float dx[4], dv[4];
 #pragma unroll
@@ -588,11 +672,29 @@ GG_DEV void mixed_advance(MixedRegs& S, const KS& K, float hf, bool& k1_valid,
   float xh[4] = {xh4.x, xh4.y, xh4.z, xh4.w}, xl[4] = {xl4.x, xl4.y, xl4.z, xl4.w};
   float vl[4] = {vl4.x, vl4.y, vl4.z, vl4.w};
   const float dx[4] = {dx4.x, dx4.y, dx4.z, dx4.w}, dv[4] = {dv4.x, dv4.y, dv4.z, dv4.w};
+#if GG_MIXED_PAIRED
+#pragma unroll
+  for (int j = 0; j < 4; j += 2) {
+    float2 h = make_float2(xh[j], xh[j + 1]), l = make_float2(xl[j], xl[j + 1]);
+    ff_add2(h, l, make_float2(dx[j], dx[j + 1]));
+    xh[j] = h.x;
+    xh[j + 1] = h.y;
+    xl[j] = l.x;
+    xl[j + 1] = l.y;
+    float2 vh2 = make_float2(S.vh[j], S.vh[j + 1]), vl2 = make_float2(vl[j], vl[j + 1]);
+    ff_add2(vh2, vl2, make_float2(dv[j], dv[j + 1]));
+    S.vh[j] = vh2.x;
+    S.vh[j + 1] = vh2.y;
+    vl[j] = vl2.x;
+    vl[j + 1] = vl2.y;
+  }
+#else
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     ff_add(xh[i], xl[i], dx[i]);
     ff_add(S.vh[i], vl[i], dv[i]);
   }
+#endif
   if (xh[3] >= kTwoPiHi) {
     ff_add(xh[3], xl[3], -kTwoPiHi);
     ff_add(xh[3], xl[3], -kTwoPiLo);
