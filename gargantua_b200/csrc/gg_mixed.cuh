@@ -44,8 +44,9 @@
 // multiply-add and the accepted step's two-sum state update with the paired
 // add, two components per instruction: 25.7 against 26.5 ms, the same bits.
 // Pairing the contraction's r and theta rows the same way (26.6 ms) or the
-// stage-6 position increments (26.2 ms) gave the same bits too but cost more
-// in register moves and spills than they saved.
+// stage-6 position increments (26.2 ms) or the polar sine and cosine's two
+// Horner chains (26.0 against 25.5 ms) gave the same bits too but cost more
+// in register moves, constant pairs and spills than they saved.
 #ifndef GG_MIXED_ERR_FP64
 #define GG_MIXED_ERR_FP64 1
 #endif
