@@ -1,11 +1,11 @@
 // gg_dual.cuh -- forward-mode dual numbers for the differentiable render.
 //
 // Dual<N> carries a value and its derivatives along N directions.  The
-// adjoint kernels (gg_adjoint.cu) use it to form the Jacobians they need --
-// of one right-hand side with respect to its stage position, velocity and
-// spin, of the crossing step, of the camera's initial state -- by running the
-// same templated physics (kerr_geometry / kerr_contract) on Dual<N> instead
-// of double.  Only the operations that code uses are defined.
+// adjoint kernels (gg_adjoint.cu) use it for the Jacobians of the crossing
+// step and of the camera's initial state, and gg_vjp.cuh for the dual form
+// of the stage product (the check beside the hand-written reverse pass), by
+// running the same templated physics (kerr_geometry / kerr_contract) on
+// Dual<N> instead of double.  Only the operations that code uses are defined.
 #pragma once
 
 #include <cuda_runtime.h>
