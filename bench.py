@@ -173,12 +173,19 @@ def barrier(world):
         dist.barrier()
 
 
+def _reduce_device() -> str:
+    """Where a reduction's tensor lives: the GPU under NCCL, the host under
+    gloo (the CPU tests of these helpers)."""
+    import torch.distributed as dist
+    return "cuda" if dist.get_backend() == "nccl" else "cpu"
+
+
 def sum_over_ranks(x: int, world: int) -> int:
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.int64, device="cuda")
+    t = torch.tensor([x], dtype=torch.int64, device=_reduce_device())
     dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return int(t.item())
 
@@ -188,7 +195,7 @@ def max_over_ranks(x: float, world: int) -> float:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=_reduce_device())
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
