@@ -49,7 +49,10 @@
 // (kerr_rhs_vjp_hand) instead of dual numbers.  GG_ADJ_STORE_K: the replay
 // keeps each accepted step's stage derivatives for the step's product instead
 // of evaluating them again.  GG_ADJ_MIN_BLOCKS: the CTAs per SM the backward's
-// registers are budgeted for (1 leaves the compiler's own choice).
+// registers are budgeted for (1 leaves the compiler's own choice).  Measured
+// on the 512^2 gradient (backward ms): dual numbers 11.2, dual with kept stages
+// 9.9, hand-written 8.5, hand-written with kept stages 7.9 (the default; the
+// forward takes 8.8); the gradients agree to 1e-15.
 #ifndef GG_ADJ_HAND_VJP
 #define GG_ADJ_HAND_VJP 1
 #endif
