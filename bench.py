@@ -66,9 +66,10 @@ METRIC = "Kerr 1080p geodesics/s, mixed-FP32 vs plain FP64 on B200 at stated end
 UNIT = "geodesics/s"
 # DRAM bytes (read + write) of one launch of the FP32 pass on the Kerr 1080p
 # frame: ncu's dram__bytes_read.sum + dram__bytes_write.sum for that launch
-# (one pass, clocks not locked).  They are the 6.2 MB image, the band queue and
-# the argument records of the once-per-ray finish and hand-off calls.
-MIXED_PASS_DRAM_BYTES = 3_556_864 + 27_299_584
+# (the second frame of a two-frame launch list, one pass, clocks not locked),
+# in the build with FP64 error sums.  They are the 6.2 MB image, the band
+# queue and the argument records of the once-per-ray finish and hand-off calls.
+MIXED_PASS_DRAM_BYTES = 3_325_440 + 43_624_448
 # Renders of this many samples or more run the mixed form's hand-back rounds
 # (kHandBackMinRays in gargantua_b200/csrc/gg_capi.cpp).
 HAND_BACK_MIN_SAMPLES = 1 << 20
