@@ -22,7 +22,11 @@ constexpr int kTraceBlock = 128;  // threads per CTA of the trace kernels
 // 26.3; the 512^2 adjoint's forward 10.1 / 8.9 / 8.6.  At 3 CTAs (168
 // registers) for the band passes and the mixed pass over returned rays, the
 // 1080p frame gains 0.3 ms but the stress frame at 2048^2 x 4 spp, whose band
-// holds 12 % of the attempts, loses 1.3 ms.  GG_TRACE_MIN_BLOCKS overrides
+// holds 12 % of the attempts, loses 1.3 ms.  The camera passes' budget (5)
+// for the band passes of renders from 2^23 samples, whose band holds enough
+// rays to be throughput-bound: 84.9 against 84.2 ms on the stress frame at
+// 2048^2 x 4 spp, 1.291 against 1.285 s at 4096^2 x 16 spp and 2.403 against
+// 2.385 s on the 2,048-scene batch, so not kept.  GG_TRACE_MIN_BLOCKS overrides
 // all three, GG_TRACE_CHAIN_MIN_BLOCKS the chain-bound one (tuning builds).
 #ifdef GG_TRACE_MIN_BLOCKS
 constexpr int kTraceMinBlocksKerr = GG_TRACE_MIN_BLOCKS;
