@@ -87,7 +87,12 @@ struct gg_ctx {
 };
 
 // Half-width (rad) of the polar caps whose attempts the mixed form runs in
-// FP64 (tuning builds override it).
+// FP64 (tuning builds override it).  Measured (mixed against FP64 DP45): the
+// stress frame at 2048^2 x 4 spp takes 84.3 / 82.1 / 81.3 ms at 0.1 / 0.05 /
+// 0.02 rad, and a Kerr a = 0.95 view from 10 deg off the axis spends 28 / 16 /
+// 9 % of its attempts in FP64 with about the same crossing errors; but on the
+// 1080p Kerr frame 0.05 rad takes the rays beyond 1e-6 from 823 to 1,056, 239
+// of them not explained by the FP64 kernel's own amplification.  So 0.1.
 #ifndef GG_POLE_BAND
 #define GG_POLE_BAND 0.1f
 #endif
