@@ -202,7 +202,7 @@ __global__ void __launch_bounds__(kTraceBlock,
 
     // ---- advance every live ray by up to kPeriod attempts -----------------
 #pragma unroll 1
-    for (int it = 0; it < kPeriod; ++it) {
+    for (int it = 0; it < (SRC == kSrcQueue ? kQueuePeriod : kPeriod); ++it) {
       if (!live) continue;
       // this lane's scene: the batch's entry, or the render's own parameters
       const DevParams& PL = BATCH ? B.scenes[scene].P : P;

@@ -27,7 +27,18 @@ constexpr unsigned kFull = 0xffffffffu;
 #ifndef GG_MIXED_PERIOD
 #define GG_MIXED_PERIOD 16
 #endif
+// The mixed form's FP64 band passes refill more often: on views whose band
+// holds many rays of uneven length the pass is throughput-bound, and idle
+// lanes cost more than ballots.  Measured (period 32 / 16 / 8 / 4 / 2): the
+// stress view at 2048^2 x 4 spp 84.1 / 82.4 / 81.9 / 82.2 / 82.8 ms, the full
+// stress frame 1.282 / 1.254 / 1.248 / 1.250 / 1.258 s, the 2,048-scene batch
+// 2.376 / 2.357 / 2.350 / 2.357 / 2.357 s; the 1080p frame, whose band pass
+// is one wave, 25.7 ms throughout.
+#ifndef GG_QUEUE_PERIOD
+#define GG_QUEUE_PERIOD 8
+#endif
 constexpr int kPeriod = GG_TRACE_PERIOD;
+constexpr int kQueuePeriod = GG_QUEUE_PERIOD;
 constexpr int kMixedPeriod = GG_MIXED_PERIOD;
 constexpr uint32_t kChunk = 32;  // samples a warp takes from the queue at once
 
