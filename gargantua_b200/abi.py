@@ -171,6 +171,7 @@ _SIGNATURES = {
     "gg_check_procedural_sky": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p]),
     "gg_check_spatial_dir": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p]),
     "gg_check_kerr_vjp": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_int, C.c_void_p]),
+    "gg_check_step_factor": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p]),
     "gg_render_batch": (C.c_int, [C.c_void_p, P(gg_scene_t), C.c_uint32, P(gg_integrator_t),
                                   P(gg_render_opts_t), C.c_void_p]),
     "gg_render_batch_device": (C.c_int, [C.c_void_p, P(gg_scene_t), C.c_uint32,

@@ -13,6 +13,7 @@
 
 #include "../../include/gargantua_gpu.h"
 #include "gg_device.cuh"
+#include "gg_mixed.cuh"
 #include "gg_vjp.cuh"
 
 namespace {
@@ -63,6 +64,13 @@ __global__ void kerr_vjp_kernel(const double* __restrict__ in, double* __restric
   }
 }
 
+__global__ void step_factor_kernel(const double* __restrict__ s2, double* __restrict__ out,
+                                   uint64_t n) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = gg::root10_8_over(s2[i]);
+}
+
 int launch_status() {
   const cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? GG_OK : GG_ERR_CUDA;
@@ -97,5 +105,15 @@ extern "C" GG_API int gg_check_kerr_vjp(const double* in_dev, double* out_dev, u
   const uint64_t blocks = (n + 127) / 128;
   kerr_vjp_kernel<<<(unsigned)(blocks < 4096 ? blocks : 4096), 128, 0,
                     static_cast<cudaStream_t>(stream)>>>(in_dev, out_dev, n, form);
+  return launch_status();
+}
+
+extern "C" GG_API int gg_check_step_factor(const double* s2_dev, double* out_dev, uint64_t n,
+                                           void* stream) {
+  if (n == 0) return GG_OK;
+  if (!s2_dev || !out_dev) return GG_ERR_INVALID_ARG;
+  const uint64_t blocks = (n + 255) / 256;
+  step_factor_kernel<<<(unsigned)(blocks < 4096 ? blocks : 4096), 256, 0,
+                       static_cast<cudaStream_t>(stream)>>>(s2_dev, out_dev, n);
   return launch_status();
 }

@@ -428,6 +428,13 @@ GG_API int gg_check_spatial_dir(const double* vel_dev, double* dirs_dev, uint64_
 GG_API int gg_check_kerr_vjp(const double* in_dev, double* out_dev, uint64_t n, int form,
                              void* stream);
 
+/* The mixed form's step-size factor of an accepted attempt, (8 / s2)^(1/10)
+ * for the squared error norm s2 (err = sqrt(s2 / 8) against tolerance 1;
+ * s2 below 8e-60 taken as 8e-60), of n values (test use; no reference
+ * counterpart; the reference's law is geodesic.rs:310-321).  Same pointer,
+ * stream and return conventions as above. */
+GG_API int gg_check_step_factor(const double* s2_dev, double* out_dev, uint64_t n, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

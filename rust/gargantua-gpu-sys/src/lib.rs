@@ -245,4 +245,6 @@ extern "C" {
                                 stream: *mut c_void) -> c_int;
     pub fn gg_check_kerr_vjp(in_dev: *const f64, out_dev: *mut f64, n: u64, form: c_int,
                              stream: *mut c_void) -> c_int;
+    pub fn gg_check_step_factor(s2_dev: *const f64, out_dev: *mut f64, n: u64,
+                                stream: *mut c_void) -> c_int;
 }
