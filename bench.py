@@ -49,6 +49,7 @@ a bounded seeded sample of the same frame.
 from __future__ import annotations
 
 import argparse
+import copy
 import ctypes as C
 import json
 import os
@@ -628,11 +629,17 @@ def measure_stress(r, side: int, spp: int, world: int, rank: int, local: int, pe
     for form, prec, stepper in (("fp64", abi.GG_PREC_FP64, abi.GG_STEPPER_REFERENCE),
                                 ("fp64_dp45", abi.GG_PREC_FP64, abi.GG_STEPPER_DP45),
                                 ("mixed", abi.GG_PREC_MIXED, abi.GG_STEPPER_DP45)):
-        warm = workloads.kerr_stress_4k(precision=prec, side=256, spp=1, stepper=stepper)
-        r.render_device(warm, img.data_ptr(), None, r.stream)
         scene = shard.shard_scene(
             workloads.kerr_stress_4k(precision=prec, side=side, spp=spp, stepper=stepper),
             rank, world)
+        # warm-up: the same frame cut to one step() call per ray, which sizes the
+        # context's per-sample buffers (the mixed form's queues: 2 x 27 GB at
+        # full size) outside the timed region; their allocation would otherwise
+        # land between the timing events
+        warm = copy.copy(scene)
+        warm.options = copy.copy(scene.options)
+        warm.options.max_steps = 1
+        r.render_device(warm, img.data_ptr(), None, r.stream)
         att = torch.empty(n_mine, dtype=torch.int32, device="cuda")
         cls = torch.empty(n_mine, dtype=torch.int32, device="cuda")
         rays = abi.gg_ray_out_t()
